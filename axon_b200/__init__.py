@@ -1,0 +1,9 @@
+"""axon_b200: B200-native engine for AXON's sparse binary assembly network.
+
+The product is ``_build/libaxon_b200.so`` (hand-written sm_100a CUDA behind the C ABI in
+``include/axon_capi.h``) and the ``_build/axon`` command line that replaces the
+reference's ``build/axon``. This package is the Python side of the same C ABI.
+"""
+from .network import CONFIG_C, Network, bstest, config, load_stim, stimuli  # noqa: F401
+
+__all__ = ["Network", "config", "CONFIG_C", "stimuli", "load_stim", "bstest"]

@@ -1,0 +1,88 @@
+"""ctypes binding of libaxon_b200.so (declarations in include/axon_capi.h).
+
+The library is built in-tree by ``axon_b200.build``; if it is missing this module raises
+instead of falling back to anything else: there is no CPU path in the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "_build" / "libaxon_b200.so"
+
+AXON_OK, AXON_EINVAL, AXON_ENOMEM, AXON_ECUDA, AXON_ETIMEOUT, AXON_ESTATE = range(6)
+
+BUF = {
+    "W0": 0, "W1": 1, "W2": 2, "W3": 3, "CONN": 4, "SPK_A": 5, "SPK_B": 6, "DRIVE": 7, "BBITS": 8,
+    "ACC": 9, "BIAS": 10, "MARG": 11, "REFBALL": 12, "DRIVELOG": 13, "MULT": 14, "STIM": 15,
+    "STATS": 16, "HIST": 17, "THETA": 18,
+}
+
+CFG_FIELDS = [
+    "ncol", "incols", "inbr", "nand", "target", "k", "ktest", "dthr", "boost", "mode", "biasup",
+    "biasdown", "biasshift", "biasdownevery", "bandlo", "bandhi", "contrast", "margingate", "hetero",
+    "ltdrep", "ltdevery", "facil", "topkpar",
+]
+
+
+class AxonCfg(C.Structure):
+    _fields_ = [(f, C.c_uint32) for f in CFG_FIELDS] + [("reserved", C.c_uint32 * 9)]
+
+
+class AxonError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"axon status {status}: {msg}")
+        self.status = status
+
+
+_lib = None
+U32P = C.POINTER(C.c_uint32)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is not built; run `python -m axon_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        L.axon_cfg_defaults.argtypes = [C.POINTER(AxonCfg)]
+        L.axon_last_error.restype = C.c_char_p
+        L.axon_create.argtypes = [C.POINTER(AxonCfg), C.c_int, C.POINTER(C.c_void_p)]
+        L.axon_destroy.argtypes = [C.c_void_p]
+        L.axon_init.argtypes = [C.c_void_p, C.c_uint32]
+        L.axon_present.argtypes = [C.c_void_p, U32P, C.c_uint32, C.c_uint32, C.c_int, C.c_int, C.c_uint32,
+                                   C.POINTER(C.c_double)]
+        L.axon_read.argtypes = [C.c_void_p, C.c_int, U32P, C.c_uint64]
+        L.axon_write.argtypes = [C.c_void_p, C.c_int, U32P, C.c_uint64]
+        L.axon_buf_words.argtypes = [C.c_void_p, C.c_int]
+        L.axon_buf_words.restype = C.c_uint64
+        L.axon_wstat.argtypes = [C.c_void_p, U32P]
+        L.axon_within.argtypes = [C.c_void_p, U32P, C.c_uint32, U32P, U32P, U32P]
+        L.axon_indeg.argtypes = [C.c_void_p, U32P]
+        L.axon_untouched.argtypes = [C.c_void_p, U32P]
+        L.axon_wdiag.argtypes = [C.c_void_p, U32P, U32P, C.c_uint32, C.c_uint32, U32P]
+        L.axon_bstest.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, U32P, U32P, U32P, U32P, U32P,
+                                  C.c_uint64]
+        L.axon_set_wait_limit.argtypes = [C.c_void_p, C.c_uint64]
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != AXON_OK:
+        raise AxonError(status, lib().axon_last_error().decode(errors="replace"))
+
+
+def u32(a: np.ndarray):
+    assert a.dtype == np.uint32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(U32P)
+
+
+def default_cfg(**kw) -> AxonCfg:
+    c = AxonCfg()
+    lib().axon_cfg_defaults(C.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, int(v))
+    return c

@@ -1,0 +1,52 @@
+// Host-side network object behind the C ABI: owns the device state of one AXON network
+// and launches the plain kernels. The reference keeps the same state in MTLBuffers
+// allocated at src/axon.mm:749-768.
+#pragma once
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/axon_capi.h"
+#include "plain.cuh"
+
+namespace axon {
+
+axon_status cuda_fail(cudaError_t e, const char* what);
+axon_status set_error(axon_status s, const std::string& msg);
+std::string validate_cfg(const axon_cfg& c);
+
+}  // namespace axon
+
+struct axon_net {
+  axon_cfg cfg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t ncol = 0, n = 0;
+  uint64_t plane_words = 0;
+  axon::NetDev d{};
+  void* base = nullptr;        // one device allocation for all buffers
+  uint32_t* hstim = nullptr;   // pinned staging for the clamp pattern
+  uint32_t* hscratch = nullptr;  // pinned staging for small reads (error word)
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  axon::LaunchShape shape{};
+  bool initialized = false;
+  uint64_t wait_ns = 2000000000ull;
+
+  axon_status create(const axon_cfg& c, int dev);
+  void release();
+  axon_status init(uint32_t seed);
+  axon_status present(const uint32_t* stim, uint32_t T, uint32_t clampSteps, bool learn, bool freeze,
+                      uint32_t useBias, double* msPerStep);
+  uint64_t buf_words(axon_buf which) const;
+  uint32_t* buf_ptr(axon_buf which) const;
+  axon_status read(axon_buf which, uint32_t* host, uint64_t words);
+  axon_status write(axon_buf which, const uint32_t* host, uint64_t words);
+  axon_status wstat(uint32_t* count);
+  axon_status within(const uint32_t* ball, uint32_t useMask, const uint32_t* postMask, const uint32_t* mult,
+                     uint32_t out[10]);
+  axon_status indeg_untouched(uint32_t which, uint32_t* out);
+  axon_status wdiag(const uint32_t* memb, const uint32_t* asmSpk, uint32_t nstim, uint32_t sel, uint32_t hist48[48]);
+  axon::PresentCfg present_cfg(uint32_t T, uint32_t clampSteps, bool learn, uint32_t useBias) const;
+  axon_status check_device_error();
+};

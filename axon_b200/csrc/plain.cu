@@ -1,0 +1,595 @@
+// Plain AXON path on sm_100a: one persistent launch runs all T steps of a presentation.
+//
+// Reference: rakib-nyc/axon src/axon.mm. There, present() (src/axon.mm:815-888) encodes
+// T x {k_drive, k_topk, k_emit, k_bias, k_learn} as five Metal dispatches per step. Here
+// the whole step loop is one cooperative launch with ONE grid barrier per step:
+//
+//   phase A  each warp owns one column (lane = neuron): drive over the column's non-silent
+//            branches (W3 tiles streamed from HBM, spikes from shared memory), the exact
+//            k-of-32 ballot, and the column drive; drive + ungated ballot are published.
+//   barrier
+//   phase B  every CTA reads all published drives/ballots (L2), selects the column
+//            threshold (the target-th largest recurrent drive) and rebuilds the whole
+//            spike vector spk(t) in its own shared memory; no second barrier is needed.
+//   phase C  each warp finishes its own column: hist/stats/driveLog records, intrinsic
+//            bias (in a register for the whole launch) and bit-serial learning on W0..W3.
+//
+// Per-neuron state that only its owner touches (bias, conn row, multiplicity) lives in
+// registers for the whole presentation; HBM traffic per step is the W3 tiles of
+// non-silent branches plus the learning read-modify-writes.
+#include <cstdint>
+
+#include "axon_device.cuh"
+#include "plain.cuh"
+
+namespace axon {
+
+// Exact selection of the column threshold over recurrent columns [incols, ncol),
+// src/axon.mm:301-352 (k_topk_par, default) and :259-292 (k_topk_serial). Both return
+// max(v, 1) where v is the need-th largest drive among drives below 2^24 when at least
+// `need` such drives exist and need >= 1; with fewer candidates both give 1; with
+// need == 0 the parallel form gives 1 and the serial form 0xFFFFFF. The selection here is
+// a radix select over the significant bits of the largest candidate; any digit split
+// yields the same order statistic.
+__device__ uint32_t block_theta(const uint32_t* sD, uint32_t incols, uint32_t ncol, uint32_t need,
+                                uint32_t topkPar, uint32_t* sHist, uint32_t* sRed) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
+  // block max and count of candidates
+  uint32_t mx = 0, cnt = 0;
+  for (uint32_t c = incols + tid; c < ncol; c += blockDim.x) {
+    const uint32_t d = sD[c];
+    if (d < (1u << 24)) { mx = max(mx, d); ++cnt; }
+  }
+  mx = __reduce_max_sync(kFull, mx);
+  cnt = __reduce_add_sync(kFull, cnt);
+  if (lane == 0) { sRed[warp] = mx; sRed[32 + warp] = cnt; }
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t m = lane < nw ? sRed[lane] : 0u, n = lane < nw ? sRed[32 + lane] : 0u;
+    m = __reduce_max_sync(kFull, m);
+    n = __reduce_add_sync(kFull, n);
+    if (lane == 0) { sRed[64] = m; sRed[65] = n; }
+  }
+  __syncthreads();
+  const uint32_t M = sRed[64], count = sRed[65];
+  if (need == 0u) return topkPar ? 1u : 0xFFFFFFu;
+  if (count < need || M == 0u) return 1u;
+
+  const uint32_t nb = 32u - __clz(M);
+  uint32_t shift = nb > 8u ? nb - 8u : 0u, hiShift = 32u;
+  uint32_t prefix = 0, rem = need;
+  const uint32_t iters = (ncol - incols + blockDim.x - 1) / blockDim.x;
+  for (;;) {
+    for (uint32_t i = tid; i < 256u; i += blockDim.x) sHist[i] = 0u;
+    __syncthreads();
+    const uint32_t width = (hiShift >= 32u ? nb : hiShift) - shift;  // <= 8
+    const uint32_t dmask = (width >= 32u) ? kFull : ((1u << width) - 1u);
+    for (uint32_t it = 0; it < iters; ++it) {
+      const uint32_t c = incols + tid + it * blockDim.x;
+      uint32_t key = kFull;
+      if (c < ncol) {
+        const uint32_t d = sD[c];
+        const bool match = hiShift >= 32u || (d >> hiShift) == (prefix >> hiShift);
+        if (d < (1u << 24) && match) key = (d >> shift) & dmask;
+      }
+      const uint32_t peers = __match_any_sync(kFull, key);
+      if (key != kFull && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&sHist[key], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t h[8], ls = 0;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) { h[i] = sHist[lane * 8 + i]; ls += h[i]; }
+      uint32_t S = ls;  // inclusive suffix sum over lanes
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t v = __shfl_down_sync(kFull, S, off);
+        if (lane + off < 32u) S += v;
+      }
+      uint32_t Snext = __shfl_down_sync(kFull, S, 1);
+      if (lane == 31u) Snext = 0u;
+      if (S >= rem && Snext < rem) {
+        uint32_t cum = Snext, b = lane * 8u, above = Snext;
+#pragma unroll
+        for (int i = 7; i >= 0; --i) {
+          if (cum + h[i] >= rem) { b = lane * 8u + i; above = cum; break; }
+          cum += h[i];
+        }
+        sRed[66] = b;
+        sRed[67] = above;
+      }
+    }
+    __syncthreads();
+    prefix |= sRed[66] << shift;
+    rem -= sRed[67];
+    __syncthreads();  // sRed reused next pass
+    if (shift == 0u) break;
+    hiShift = shift;
+    shift = shift >= 8u ? shift - 8u : 0u;
+  }
+  return max(prefix, 1u);
+}
+
+// One 32-synapse word of k_learn's update, src/axon.mm:466-488: co-active pairs are
+// potentiated (phase 1), depressed ltdRep times (phase 2) or take the legacy rule
+// (phase 0); optional heterosynaptic LTD; then the clip band on every lane.
+__device__ __forceinline__ void learn_word(uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t& a3, uint32_t sp,
+                                           bool want, uint32_t phase, uint32_t t, const PresentCfg& c,
+                                           uint32_t& nLTP, uint32_t& nLTD) {
+  const uint32_t co = want ? sp : 0u;
+  if (phase == 1u) {
+    bs_inc(a0, a1, a2, a3, co);
+    nLTP += __popc(co);
+  } else if (phase == 2u) {
+    for (uint32_t r = 0; r < c.ltdRep; ++r) bs_dec(a0, a1, a2, a3, co);
+    nLTD += __popc(co) * c.ltdRep;
+  } else {
+    bs_inc(a0, a1, a2, a3, co);
+    bs_dec(a0, a1, a2, a3, (want && (t % 2u == 1u)) ? ~sp : 0u);
+  }
+  if (c.hetero != 0u && phase == 1u) bs_dec(a0, a1, a2, a3, want ? ~sp : 0u);
+  if (c.bandHi != 0u) bs_clip(a0, a1, a2, a3, c.bandLo, c.bandHi);
+}
+
+template <int CPW>
+__global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  const uint32_t ncol = c.ncol, incols = c.incols;
+  const uint32_t ngrp = ncol / 8u, nactw = (((ngrp + 31u) / 32u) + 3u) & ~3u;  // 16-byte multiple
+  uint32_t* sSpk0 = sm;                    // spike vectors, ping-pong
+  uint32_t* sSpk1 = sm + ncol;
+  uint32_t* sAct0 = sm + 2 * ncol;         // group-activity bits, ping-pong
+  uint32_t* sAct1 = sAct0 + nactw;
+  uint32_t* sD = sAct1 + nactw;            // staged drives of the current step
+  uint32_t* sB = sD + ncol;                // staged ungated ballots
+  uint32_t* sStim = sB + ncol;             // input clamp pattern
+  uint32_t* sHist = sStim + ((incols + 3u) & ~3u);
+  uint32_t* sRed = sHist + 256;            // 96 words of reduction scratch
+  uint32_t* sFlag = sRed + 96;
+
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, wpb = blockDim.x >> 5;
+  const uint32_t gwarp = blockIdx.x * wpb + warp, nwarps = gridDim.x * wpb;
+
+  for (uint32_t i = tid; i < ncol; i += blockDim.x) sSpk0[i] = 0u;
+  for (uint32_t i = tid; i < nactw; i += blockDim.x) sAct0[i] = 0u;
+  for (uint32_t i = tid; i < incols; i += blockDim.x) sStim[i] = d.stim[i];
+
+  // per-column state of the columns this warp owns (lane = neuron, or lane = branch for conn)
+  uint32_t col[CPW], cn[CPW], bias[CPW], mul[CPW], refb[CPW], acc[CPW], bb[CPW], ball[CPW], vk[CPW], vk1[CPW], drv[CPW];
+#pragma unroll
+  for (int i = 0; i < CPW; ++i) {
+    col[i] = gwarp + (uint32_t)i * nwarps;
+    cn[i] = bias[i] = mul[i] = refb[i] = acc[i] = bb[i] = ball[i] = vk[i] = vk1[i] = drv[i] = 0u;
+    if (col[i] < ncol) {
+      cn[i] = d.conn[col[i] * kNslot + lane];
+      bias[i] = d.bias[col[i] * 32u + lane];
+      mul[i] = d.mult[col[i] * 32u + lane];
+      refb[i] = d.refBall[col[i]];
+    }
+  }
+  __syncthreads();
+
+  for (uint32_t t = 0; t < c.T; ++t) {
+    const uint32_t* sIn = (t & 1u) ? sSpk1 : sSpk0;
+    uint32_t* sOut = (t & 1u) ? sSpk0 : sSpk1;
+    const uint32_t* sActIn = (t & 1u) ? sAct1 : sAct0;
+    uint32_t* sActOut = (t & 1u) ? sAct0 : sAct1;
+    const uint4* sIn4 = reinterpret_cast<const uint4*>(sIn);
+    const uint32_t par = t & 1u;
+    const bool clamp = t < c.clampSteps;
+    const uint32_t phase = (!c.learn || !c.contrast) ? 0u
+                           : (clamp ? 1u : (((t - c.clampSteps) % c.ltdEvery == 0u) ? 2u : 3u));
+
+    // ---------------- phase A: drive (k_drive, src/axon.mm:150-190) + ungated k-WTA
+#pragma unroll
+    for (int i = 0; i < CPW; ++i) {
+      if (col[i] >= ncol) continue;  // warp-uniform
+      const uint32_t cc = col[i];
+      uint32_t active = __ballot_sync(kFull, (sActIn[cn[i] >> 5] >> (cn[i] & 31u)) & 1u);
+      uint32_t a = 0, b2 = 0;
+      const uint4* Wt = d.W3 + (size_t)cc * kNslot * kTileU4 + lane;
+      while (active) {
+        uint32_t s[4];
+        bool v[4];
+        uint4 w0[4], w1[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          v[u] = active != 0u;
+          s[u] = v[u] ? (uint32_t)(__ffs(active) - 1) : 0u;
+          active &= active - 1u;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (v[u]) {
+            w0[u] = __ldcg(Wt + s[u] * kTileU4);
+            w1[u] = __ldcg(Wt + s[u] * kTileU4 + 32);
+          }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (v[u]) {
+            const uint32_t g = __shfl_sync(kFull, cn[i], s[u]);
+            const uint32_t cnt = popc4(w0[u], sIn4[2 * g]) + popc4(w1[u], sIn4[2 * g + 1]);
+            const bool nmda = cnt >= c.dthr;
+            if (nmda) b2 |= 1u << s[u];
+            if (c.mode == 0u) a += cnt;
+            else if (c.mode == 1u) a += nmda ? cnt + c.boost : cnt;
+            else a += nmda ? 1u : 0u;
+          }
+      }
+      if (c.facil != 0u && ((sIn[cc] >> lane) & 1u)) a += c.facil;
+      const uint32_t bi = c.useBias ? (bias[i] >> c.biasShift) : 0u;
+      a = a > bi ? a - bi : 0u;
+      acc[i] = a;
+      bb[i] = b2;
+      drv[i] = __reduce_add_sync(kFull, a);
+      ball[i] = warp_kwta(a, lane, c.k, vk[i], vk1[i]);
+      if (lane == 0) {
+        __stcg(d.xdrive + par * ncol + cc, drv[i]);
+        __stcg(d.xball + par * ncol + cc, ball[i]);
+      }
+    }
+
+    if (!grid_barrier(d.bar, d.err, gridDim.x, t, c.waitNs, sFlag)) return;
+
+    // ---------------- phase B: column threshold (k_topk) and the full spike vector
+    for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x) {
+      reinterpret_cast<uint4*>(sD)[i] = __ldcg(reinterpret_cast<const uint4*>(d.xdrive + par * ncol) + i);
+      reinterpret_cast<uint4*>(sB)[i] = __ldcg(reinterpret_cast<const uint4*>(d.xball + par * ncol) + i);
+    }
+    __syncthreads();
+    const uint32_t theta = block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed);
+    const uint32_t gate = max(theta, 1u);
+    // k_emit gate and clamp, src/axon.mm:211-212
+    for (uint32_t cc = tid; cc < ncol; cc += blockDim.x) {
+      uint32_t b = sD[cc] < gate ? 0u : sB[cc];
+      if (clamp && cc < incols) b = sStim[cc];
+      sOut[cc] = b;
+    }
+    __syncthreads();
+    for (uint32_t gb = warp * 32u; gb < ngrp; gb += wpb * 32u) {
+      const uint32_t g = gb + lane;
+      bool any = false;
+      if (g < ngrp) {
+        const uint4 p = reinterpret_cast<const uint4*>(sOut)[2 * g], q = reinterpret_cast<const uint4*>(sOut)[2 * g + 1];
+        any = (p.x | p.y | p.z | p.w | q.x | q.y | q.z | q.w) != 0u;
+      }
+      const uint32_t wv = __ballot_sync(kFull, any);
+      if (lane == 0) sActOut[gb >> 5] = wv;
+    }
+    if (blockIdx.x == 0 && tid == 0) { d.theta[0] = theta; d.theta[1] = 0u; }
+
+    // ---------------- phase C: own-column records, bias and learning
+#pragma unroll
+    for (int i = 0; i < CPW; ++i) {
+      if (col[i] >= ncol) continue;
+      const uint32_t cc = col[i];
+      const uint32_t b = sOut[cc];
+      const bool recur = cc >= incols;
+      const bool fired = (b >> lane) & 1u;
+      if (recur) {
+        // stats[2] and driveLog, src/axon.mm:213-220
+        const uint32_t coinc = __reduce_add_sync(kFull, fired ? (uint32_t)__popc(bb[i]) : 0u);
+        const bool member = (refb[i] >> lane) & 1u;
+        const bool shared = mul[i] > 1u;
+        const uint32_t mS = __ballot_sync(kFull, member && shared), mE = __ballot_sync(kFull, member && !shared);
+        const uint32_t sumS = __reduce_add_sync(kFull, (member && shared) ? acc[i] : 0u);
+        const uint32_t sumE = __reduce_add_sync(kFull, (member && !shared) ? acc[i] : 0u);
+        if (lane == 0) {
+          if (coinc) atomicAdd(d.stats + 2, coinc);
+          if (mS) { atomicAdd(d.driveLog + t * 4u + 0u, sumS); atomicAdd(d.driveLog + t * 4u + 1u, (uint32_t)__popc(mS)); }
+          if (mE) { atomicAdd(d.driveLog + t * 4u + 2u, sumE); atomicAdd(d.driveLog + t * 4u + 3u, (uint32_t)__popc(mE)); }
+        }
+      }
+      if (lane == 0) {
+        d.hist[(size_t)t * ncol + cc] = b;
+        if (b != 0u && recur) {  // src/axon.mm:225-234
+          const uint32_t sb = 64u + t * 8u;
+          atomicAdd(d.stats + 0, 1u);
+          atomicAdd(d.stats + 1, (uint32_t)__popc(b));
+          atomicAdd(d.stats + sb + 0u, vk[i] - vk1[i]);
+          atomicAdd(d.stats + sb + 1u, vk[i]);
+          atomicAdd(d.stats + sb + 2u, 1u);
+          if (vk[i] == vk1[i]) atomicAdd(d.stats + sb + 3u, 1u);
+          if (vk[i] == 0u) atomicAdd(d.stats + sb + 4u, 1u);
+        }
+      }
+      if (!c.learn) continue;
+      // k_bias, src/axon.mm:240-253
+      if (recur) {
+        const int dec = ((t % max(c.biasDownEvery, 1u)) == 0u) ? (int)c.biasDown : 0;
+        const int nb = (int)bias[i] + (fired ? (int)c.biasUp : -dec);
+        bias[i] = (uint32_t)max(0, nb);
+      }
+      // k_learn, src/axon.mm:436-495
+      if (phase == 3u || b == 0u) continue;
+      if (c.marginGate != 0u && !(vk[i] > vk1[i])) continue;
+      const uint32_t vmask = __reduce_or_sync(kFull, fired ? bb[i] : 0u);
+      uint32_t nLTP = 0, nLTD = 0;
+      uint32_t rem = vmask;
+      while (rem) {
+        const uint32_t s = (uint32_t)(__ffs(rem) - 1);
+        rem &= rem - 1u;
+        const bool want = fired && ((bb[i] >> s) & 1u);
+        const uint32_t g = __shfl_sync(kFull, cn[i], s);
+        const size_t base = ((size_t)cc * kNslot + s) * kTileU4 + lane;
+        uint4 p0[2], p1[2], p2[2], p3[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          p0[j] = __ldcg(d.W0 + base + 32 * j);
+          p1[j] = __ldcg(d.W1 + base + 32 * j);
+          p2[j] = __ldcg(d.W2 + base + 32 * j);
+          p3[j] = __ldcg(d.W3 + base + 32 * j);
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const uint4 sp4 = sIn4[2 * g + j];
+          learn_word(p0[j].x, p1[j].x, p2[j].x, p3[j].x, sp4.x, want, phase, t, c, nLTP, nLTD);
+          learn_word(p0[j].y, p1[j].y, p2[j].y, p3[j].y, sp4.y, want, phase, t, c, nLTP, nLTD);
+          learn_word(p0[j].z, p1[j].z, p2[j].z, p3[j].z, sp4.z, want, phase, t, c, nLTP, nLTD);
+          learn_word(p0[j].w, p1[j].w, p2[j].w, p3[j].w, sp4.w, want, phase, t, c, nLTP, nLTD);
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          __stcg(d.W0 + base + 32 * j, p0[j]);
+          __stcg(d.W1 + base + 32 * j, p1[j]);
+          __stcg(d.W2 + base + 32 * j, p2[j]);
+          __stcg(d.W3 + base + 32 * j, p3[j]);
+        }
+      }
+      const uint32_t sLTP = __reduce_add_sync(kFull, nLTP), sLTD = __reduce_add_sync(kFull, nLTD);
+      const uint32_t kLTP = __popc(__ballot_sync(kFull, nLTP != 0u)), kLTD = __popc(__ballot_sync(kFull, nLTD != 0u));
+      if (lane == 0) {
+        if (sLTP) atomicAdd(d.stats + 8, sLTP);
+        if (sLTD) atomicAdd(d.stats + 9, sLTD);
+        if (kLTP) atomicAdd(d.stats + 10, kLTP);
+        if (kLTD) atomicAdd(d.stats + 11, kLTD);
+      }
+    }
+    __syncthreads();  // sOut / sActOut complete before the next step reads them
+  }
+
+  // ---------------- final state, as the reference's buffers hold it after present()
+  const uint32_t T = c.T;
+  const uint32_t* sLast = (T & 1u) ? sSpk1 : sSpk0;   // spk(T-1)
+  const uint32_t* sPrev = (T & 1u) ? sSpk0 : sSpk1;   // spk(T-2), zero when T == 1
+  uint32_t* gLast = ((T - 1u) & 1u) ? d.spkA : d.spkB;
+  uint32_t* gPrev = ((T - 1u) & 1u) ? d.spkB : d.spkA;
+#pragma unroll
+  for (int i = 0; i < CPW; ++i) {
+    if (col[i] >= ncol) continue;
+    const uint32_t cc = col[i];
+    d.acc[cc * 32u + lane] = acc[i];
+    d.bbits[cc * 32u + lane] = bb[i];
+    if (c.learn) d.bias[cc * 32u + lane] = bias[i];
+    if (lane == 0) {
+      d.drive[cc] = drv[i];
+      d.marg[cc] = vk[i] > vk1[i] ? 1u : 0u;
+      gLast[cc] = sLast[cc];
+      gPrev[cc] = T >= 2u ? sPrev[cc] : 0u;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- launch helpers
+size_t present_smem_bytes(uint32_t ncol, uint32_t incols) {
+  const uint32_t ngrp = ncol / 8u, nactw = (((ngrp + 31u) / 32u) + 3u) & ~3u;
+  const size_t words = 2ull * ncol + 2ull * nactw + 2ull * ncol + ((incols + 3u) & ~3u) + 256 + 96 + 4;
+  return words * 4;
+}
+
+cudaError_t launch_present(const NetDev& d, const PresentCfg& c, const LaunchShape& ls, cudaStream_t st) {
+  void* args[] = {(void*)&d, (void*)&c};
+  const void* fn = nullptr;
+  switch (ls.cpw) {
+    case 1: fn = (const void*)k_present<1>; break;
+    case 2: fn = (const void*)k_present<2>; break;
+    case 4: fn = (const void*)k_present<4>; break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaLaunchCooperativeKernel(fn, dim3(ls.grid), dim3(ls.wpb * 32), args, ls.smem, st);
+}
+
+cudaError_t present_max_blocks_per_sm(int cpw, int threads, size_t smem, int* out) {
+  const void* fn = nullptr;
+  switch (cpw) {
+    case 1: fn = (const void*)k_present<1>; break;
+    case 2: fn = (const void*)k_present<2>; break;
+    case 4: fn = (const void*)k_present<4>; break;
+    default: return cudaErrorInvalidValue;
+  }
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, fn, threads, smem);
+}
+
+// ---------------------------------------------------------------- init kernels
+// k_init_w, src/axon.mm:86-104: one thread per uint4 of each plane.
+__global__ void k_init_w(uint4* W0, uint4* W1, uint4* W2, uint4* W3, uint32_t nAnd, uint32_t seed, uint64_t nU4) {
+  const uint64_t gg = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gg >= nU4) return;
+  const uint32_t g = (uint32_t)gg ^ (seed * 0x9E3779B9u);
+  uint32_t m0 = kFull, m1 = kFull, m2 = kFull, m3 = kFull;
+  for (uint32_t i = 0; i < nAnd; ++i) {
+    m0 &= hash32(g * 32u + i * 4u + 0u);
+    m1 &= hash32(g * 32u + i * 4u + 1u);
+    m2 &= hash32(g * 32u + i * 4u + 2u);
+    m3 &= hash32(g * 32u + i * 4u + 3u);
+  }
+  const uint4 m = make_uint4(m0, m1, m2, m3);
+  const uint4 cc = make_uint4(hash32(g * 8u + 11u), hash32(g * 8u + 13u), hash32(g * 8u + 17u), hash32(g * 8u + 19u));
+  W3[gg] = m;
+  W2[gg] = make_uint4(~m.x | cc.x, ~m.y | cc.y, ~m.z | cc.z, ~m.w | cc.w);
+  W1[gg] = cc;
+  W0[gg] = make_uint4(~cc.x, ~cc.y, ~cc.z, ~cc.w);
+}
+// k_init_conn, src/axon.mm:109-117
+__global__ void k_init_conn(uint32_t* conn, uint32_t nGrp, uint32_t nInGrp, uint32_t inBr, uint32_t seed, uint32_t n) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const uint32_t s = g % kNslot;
+  const uint32_t h = hash32(g * 2246822519u + 7u + seed * 2654435761u);
+  conn[g] = (s < inBr) ? (h % nInGrp) : (nInGrp + h % (nGrp - nInGrp));
+}
+
+cudaError_t launch_init(const NetDev& d, uint32_t ncol, uint32_t incols, uint32_t inbr, uint32_t nand, uint32_t seed,
+                        cudaStream_t st) {
+  const uint64_t nU4 = (uint64_t)ncol * kNslot * kTileU4;
+  k_init_w<<<(unsigned)((nU4 + 255) / 256), 256, 0, st>>>(d.W0, d.W1, d.W2, d.W3, nand, seed, nU4);
+  const uint32_t n = ncol * kNslot;
+  k_init_conn<<<(n + 255) / 256, 256, 0, st>>>(d.conn, ncol / 8u, incols / 8u, inbr, seed, n);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- diagnostics
+// k_wstat, src/axon.mm:641-646
+__global__ void k_wstat(const uint4* W3, uint64_t nU4, uint32_t* out) {
+  uint32_t s = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nU4; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint4 w = __ldcs(W3 + i);
+    s += __popc(w.x) + __popc(w.y) + __popc(w.z) + __popc(w.w);
+  }
+  s = __reduce_add_sync(kFull, s);
+  if ((threadIdx.x & 31u) == 0u) atomicAdd(out, s);
+}
+
+// k_within, src/axon.mm:524-562: warp per column, lane per postsynaptic neuron.
+__global__ void k_within(const uint4* W3, const uint32_t* conn, const uint32_t* ball, uint32_t inBr, uint32_t inCols,
+                         uint32_t ncol, uint32_t useMask, const uint32_t* postMask, const uint32_t* mult, uint32_t* out) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t colw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (colw >= ncol || colw < inCols) return;
+  const uint32_t gid = colw * 32u + lane;
+  bool sel = useMask ? (postMask[gid] != 0u) : (((ball[colw] >> lane) & 1u) != 0u);
+  uint32_t fIn = 0, pIn = 0, fOut = 0, pOut = 0;
+  if (sel) {
+    const uint4* ballV = reinterpret_cast<const uint4*>(ball);
+    for (uint32_t s = inBr; s < kNslot; ++s) {
+      const uint32_t g = conn[colw * kNslot + s];
+      for (uint32_t j = 0; j < 2; ++j) {
+        const uint4 ap = ballV[2 * g + j];
+        const uint4 w = W3[((size_t)colw * kNslot + s) * kTileU4 + 32 * j + lane];
+        fIn += popc4(w, ap);
+        pIn += __popc(ap.x) + __popc(ap.y) + __popc(ap.z) + __popc(ap.w);
+        const uint4 nap = make_uint4(~ap.x, ~ap.y, ~ap.z, ~ap.w);
+        fOut += popc4(w, nap);
+        pOut += __popc(nap.x) + __popc(nap.y) + __popc(nap.z) + __popc(nap.w);
+      }
+    }
+    atomicAdd(out + 0, fIn); atomicAdd(out + 1, pIn); atomicAdd(out + 2, fOut); atomicAdd(out + 3, pOut);
+    const uint32_t m = mult ? mult[gid] : 0u;
+    const uint32_t b = m > 1u ? 4u : 6u;
+    atomicAdd(out + b, fIn); atomicAdd(out + b + 1, pIn);
+    atomicAdd(out + (m > 1u ? 8u : 9u), 1u);
+  }
+}
+
+// k_indeg, src/axon.mm:566-581 and k_untouched, src/axon.mm:501-519 (which = 0 / 1)
+__global__ void k_indeg_untouched(const uint4* W0, const uint4* W1, const uint4* W2, const uint4* W3, uint32_t inBr,
+                                  uint32_t ncol, uint32_t which, uint32_t* out) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t colw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (colw >= ncol) return;
+  uint32_t r = 0;
+  for (uint32_t s = inBr; s < kNslot; ++s)
+    for (uint32_t j = 0; j < 2; ++j) {
+      const size_t idx = ((size_t)colw * kNslot + s) * kTileU4 + 32 * j + lane;
+      const uint4 a3 = W3[idx];
+      if (which == 0u) {
+        r += __popc(a3.x) + __popc(a3.y) + __popc(a3.z) + __popc(a3.w);
+      } else {
+        const uint4 a0 = W0[idx], a1 = W1[idx], a2 = W2[idx];
+        const uint32_t x[4] = {a0.x, a0.y, a0.z, a0.w}, y[4] = {a1.x, a1.y, a1.z, a1.w},
+                       z[4] = {a2.x, a2.y, a2.z, a2.w}, w[4] = {a3.x, a3.y, a3.z, a3.w};
+        for (int q = 0; q < 4; ++q) {
+          const uint32_t v5 = ~w[q] & z[q] & ~y[q] & x[q], v6 = ~w[q] & z[q] & y[q] & ~x[q];
+          r += __popc(v5 | v6);
+        }
+      }
+    }
+  out[colw * 32u + lane] = r;
+}
+
+// k_wdiag, src/axon.mm:591-638
+__global__ void k_wdiag(const uint4* W0, const uint4* W1, const uint4* W2, const uint4* W3, const uint32_t* conn,
+                        const uint32_t* memb, const uint32_t* asmSpk, uint32_t nstim, uint32_t inBr, uint32_t sel,
+                        uint32_t ncol, uint32_t* hist) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t colw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (colw >= ncol) return;
+  const uint32_t mypost = memb[colw * 32u + lane];
+  if (mypost == 0u) return;
+  uint32_t acc[48];
+  for (int i = 0; i < 48; ++i) acc[i] = 0u;
+  for (uint32_t s = 0; s < kNslot; ++s) {
+    const bool isAff = s < inBr;
+    if (sel == 0u && isAff) continue;
+    if (sel == 1u && !isAff) continue;
+    const uint32_t g = conn[colw * kNslot + s];
+    for (uint32_t j = 0; j < 2; ++j) {
+      const size_t idx = ((size_t)colw * kNslot + s) * kTileU4 + 32 * j + lane;
+      const uint4 A0 = W0[idx], A1 = W1[idx], A2 = W2[idx], A3 = W3[idx];
+      const uint32_t a0[4] = {A0.x, A0.y, A0.z, A0.w}, a1[4] = {A1.x, A1.y, A1.z, A1.w},
+                     a2[4] = {A2.x, A2.y, A2.z, A2.w}, a3[4] = {A3.x, A3.y, A3.z, A3.w};
+      for (int q = 0; q < 4; ++q) {
+        uint32_t within = 0, anyp = 0;
+        for (uint32_t qq = 0; qq < nstim; ++qq) {
+          const uint32_t ap = asmSpk[(size_t)qq * ncol + 8u * g + 4u * j + q];
+          anyp |= ap;
+          if ((mypost >> qq) & 1u) within |= ap;
+        }
+        const uint32_t between = anyp & ~within;
+        for (uint32_t v = 0; v < 16u; ++v) {
+          const uint32_t eq = ((v & 1u) ? a0[q] : ~a0[q]) & ((v & 2u) ? a1[q] : ~a1[q]) & ((v & 4u) ? a2[q] : ~a2[q]) &
+                              ((v & 8u) ? a3[q] : ~a3[q]);
+          acc[v] += __popc(eq & within);
+          acc[16 + v] += __popc(eq & between);
+          acc[32 + v] += __popc(eq);
+        }
+      }
+    }
+  }
+  for (int i = 0; i < 48; ++i)
+    if (acc[i]) atomicAdd(hist + i, acc[i]);
+}
+
+// k_bstest, src/axon.mm:424-434: one thread per 32-synapse word
+__global__ void k_bstest(uint32_t* A0, uint32_t* A1, uint32_t* A2, uint32_t* A3, const uint32_t* M, uint32_t op,
+                         uint32_t lo, uint32_t hi, uint64_t n) {
+  const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  uint32_t a0 = A0[g], a1 = A1[g], a2 = A2[g], a3 = A3[g];
+  if (op == 0u) bs_inc(a0, a1, a2, a3, M[g]);
+  else if (op == 1u) bs_dec(a0, a1, a2, a3, M[g]);
+  else bs_clip(a0, a1, a2, a3, lo, hi);
+  A0[g] = a0; A1[g] = a1; A2[g] = a2; A3[g] = a3;
+}
+
+cudaError_t launch_wstat(const NetDev& d, uint32_t ncol, uint32_t* out, cudaStream_t st) {
+  const uint64_t nU4 = (uint64_t)ncol * kNslot * kTileU4;
+  k_wstat<<<148 * 8, 256, 0, st>>>(d.W3, nU4, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_within(const NetDev& d, uint32_t ncol, uint32_t inBr, uint32_t inCols, const uint32_t* ball,
+                          uint32_t useMask, const uint32_t* postMask, const uint32_t* mult, uint32_t* out,
+                          cudaStream_t st) {
+  k_within<<<(ncol * 32 + 255) / 256, 256, 0, st>>>(d.W3, d.conn, ball, inBr, inCols, ncol, useMask, postMask, mult, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_indeg_untouched(const NetDev& d, uint32_t ncol, uint32_t inBr, uint32_t which, uint32_t* out,
+                                   cudaStream_t st) {
+  k_indeg_untouched<<<(ncol * 32 + 255) / 256, 256, 0, st>>>(d.W0, d.W1, d.W2, d.W3, inBr, ncol, which, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_wdiag(const NetDev& d, uint32_t ncol, const uint32_t* memb, const uint32_t* asmSpk, uint32_t nstim,
+                         uint32_t inBr, uint32_t sel, uint32_t* hist, cudaStream_t st) {
+  k_wdiag<<<(ncol * 32 + 127) / 128, 128, 0, st>>>(d.W0, d.W1, d.W2, d.W3, d.conn, memb, asmSpk, nstim, inBr, sel, ncol,
+                                                  hist);
+  return cudaGetLastError();
+}
+cudaError_t launch_bstest(uint32_t* a0, uint32_t* a1, uint32_t* a2, uint32_t* a3, const uint32_t* m, uint32_t op,
+                          uint32_t lo, uint32_t hi, uint64_t n, cudaStream_t st) {
+  k_bstest<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a0, a1, a2, a3, m, op, lo, hi, n);
+  return cudaGetLastError();
+}
+
+}  // namespace axon

@@ -1,0 +1,141 @@
+"""Python mirror of the reference's engine state machine over the C ABI.
+
+``Network`` holds one AXON network on a GPU. Its methods are the reference's device
+operations (src/axon.mm): ``init`` = k_init_w + k_init_conn, ``present`` = present(),
+``wstat`` = k_wstat, ``within`` = k_within, ``indeg`` = k_indeg, ``untouched`` =
+k_untouched, ``wdiag`` = k_wdiag. Buffers are read and written by the reference's
+MTLBuffer names (``read("W3")``, ``write("REFBALL", ...)``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi as A
+
+
+def config(**kw) -> A.AxonCfg:
+    """Reference CLI defaults (src/axon.mm:688-731) overridden by ``kw`` (CLI key names)."""
+    return A.default_cfg(**kw)
+
+
+CONFIG_C = dict(nand=4, target=64, k=24, dthr=1, mode=1, inbr=4, contrast=1, margingate=0, ltdrep=1,
+                ltdevery=2, biasup=73, biasdown=1)
+
+
+class Network:
+    def __init__(self, cfg: A.AxonCfg | dict | None = None, device: int = 0):
+        if cfg is None or isinstance(cfg, dict):
+            cfg = config(**(cfg or {}))
+        self.cfg = cfg
+        self.ncol = cfg.ncol
+        self.n = cfg.ncol * 32
+        h = C.c_void_p()
+        A.check(A.lib().axon_create(C.byref(cfg), device, C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if self._h:
+            A.lib().axon_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state machine
+    def init(self, seed: int) -> None:
+        A.check(A.lib().axon_init(self._h, seed))
+
+    def present(self, stim: np.ndarray, T: int, clamp_steps: int, learn: bool, freeze: bool = False,
+                use_bias: int = 2) -> float:
+        stim = np.ascontiguousarray(stim, dtype=np.uint32)
+        assert stim.shape == (self.ncol,)
+        ms = C.c_double()
+        A.check(A.lib().axon_present(self._h, A.u32(stim), T, clamp_steps, int(learn), int(freeze), use_bias,
+                                     C.byref(ms)))
+        return ms.value
+
+    def set_wait_limit(self, ns: int) -> None:
+        A.check(A.lib().axon_set_wait_limit(self._h, ns))
+
+    # -- buffers
+    def words(self, name: str) -> int:
+        return int(A.lib().axon_buf_words(self._h, A.BUF[name]))
+
+    def read(self, name: str) -> np.ndarray:
+        out = np.empty(self.words(name), dtype=np.uint32)
+        A.check(A.lib().axon_read(self._h, A.BUF[name], A.u32(out), out.size))
+        return out
+
+    def write(self, name: str, arr: np.ndarray) -> None:
+        arr = np.ascontiguousarray(arr, dtype=np.uint32)
+        A.check(A.lib().axon_write(self._h, A.BUF[name], A.u32(arr), arr.size))
+
+    def final_spikes(self, T: int) -> np.ndarray:
+        """The spike buffer present() wrote last (spkB after an odd T, spkA after an even T)."""
+        return self.read("SPK_B" if (T & 1) else "SPK_A")
+
+    # -- diagnostics
+    def wstat(self) -> int:
+        v = C.c_uint32()
+        A.check(A.lib().axon_wstat(self._h, C.byref(v)))
+        return v.value
+
+    def within(self, ball: np.ndarray, use_mask: int = 0, post_mask: np.ndarray | None = None,
+               mult: np.ndarray | None = None) -> np.ndarray:
+        ball = np.ascontiguousarray(ball, dtype=np.uint32)
+        out = np.zeros(10, dtype=np.uint32)
+        pm = A.u32(np.ascontiguousarray(post_mask, dtype=np.uint32)) if post_mask is not None else None
+        mu = A.u32(np.ascontiguousarray(mult, dtype=np.uint32)) if mult is not None else None
+        A.check(A.lib().axon_within(self._h, A.u32(ball), use_mask, pm, mu, A.u32(out)))
+        return out
+
+    def indeg(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.uint32)
+        A.check(A.lib().axon_indeg(self._h, A.u32(out)))
+        return out
+
+    def untouched(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.uint32)
+        A.check(A.lib().axon_untouched(self._h, A.u32(out)))
+        return out
+
+    def wdiag(self, memb: np.ndarray, asm_spk: np.ndarray, nstim: int, sel: int) -> np.ndarray:
+        out = np.zeros(48, dtype=np.uint32)
+        A.check(A.lib().axon_wdiag(self._h, A.u32(np.ascontiguousarray(memb, dtype=np.uint32)),
+                                   A.u32(np.ascontiguousarray(asm_spk, dtype=np.uint32)), nstim, sel, A.u32(out)))
+        return out
+
+
+def stimuli(seed: int, nstim: int, incols: int, stimcols: int) -> np.ndarray:
+    """Input patterns of the reference protocol (src/axon.mm:793-799), shape (nstim, stimcols)."""
+    out = np.empty(nstim * stimcols, dtype=np.uint32)
+    A.check(A.lib().axon_stimuli(seed, nstim, incols, stimcols, A.u32(out)))
+    return out.reshape(nstim, stimcols)
+
+
+def load_stim(cols: np.ndarray, keep: float, seed: int, ncol: int) -> np.ndarray:
+    """Clamp words of one presentation (loadStim, src/axon.mm:800-804)."""
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    out = np.empty(ncol, dtype=np.uint32)
+    A.check(A.lib().axon_load_stim(A.u32(cols), cols.size, C.c_double(keep), seed, ncol, A.u32(out)))
+    return out
+
+
+def bstest(op: int, lo: int, hi: int, planes: list[np.ndarray], mask: np.ndarray, device: int = 0) -> None:
+    """Runs the bit-serial inc/dec/clip kernel in place on four planes (k_bstest)."""
+    ps = [np.ascontiguousarray(p, dtype=np.uint32) for p in planes]
+    m = np.ascontiguousarray(mask, dtype=np.uint32)
+    A.check(A.lib().axon_bstest(device, op, lo, hi, *(A.u32(p) for p in ps), A.u32(m), m.size))
+    for dst, src in zip(planes, ps):
+        dst[...] = src

@@ -1,0 +1,150 @@
+/*
+ * axon_capi.h - C ABI of the B200 AXON engine (libaxon_b200.so).
+ *
+ * rakib-nyc/axon has no library API: its boundary is the `build/axon key=value` CLI
+ * (src/axon.mm:660-735) and the lines it prints. Internally every stage is one Metal
+ * dispatch bound to fixed buffer slots and a 26-word Params block (src/axon.mm:56-83,
+ * 650-652). This header exposes the same state machine as plain C entry points so the
+ * engine's own CLI (the drop-in for build/axon), tests and other hosts can drive it:
+ * each function below names the reference routine it replaces.
+ *
+ * Conventions: all arrays are host memory owned by the caller and copied by the call;
+ * sizes are element counts of uint32_t unless stated. No call exits the process: every
+ * failure is an axon_status. One host thread per axon_net at a time.
+ */
+#ifndef AXON_CAPI_H
+#define AXON_CAPI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum axon_status {
+  AXON_OK = 0,
+  AXON_EINVAL = 1,   /* bad argument or configuration */
+  AXON_ENOMEM = 2,   /* device or pinned host allocation failed */
+  AXON_ECUDA = 3,    /* a CUDA runtime call failed */
+  AXON_ETIMEOUT = 4, /* a grid-wide wait in a persistent kernel gave up; the kernel exited */
+  AXON_ESTATE = 5    /* call out of order (e.g. present before init) */
+} axon_status;
+
+/* Network configuration. Field meaning and reference defaults follow the CLI keys of
+ * src/axon.mm:688-735 (key name in brackets). `bandhi` is the key value: the engine
+ * applies it only when `contrast` != 0, as src/axon.mm:812 does. */
+typedef struct axon_cfg {
+  uint32_t ncol;          /* [ncol] columns of 32 neurons, multiple of 32, <= 16384 */
+  uint32_t incols;        /* [incols] clamped input columns */
+  uint32_t inbr;          /* [inbr] afferent branches of 32 */
+  uint32_t nand;          /* [nand] initial functional density 2^-nand */
+  uint32_t target;        /* [target] active columns (top-K) */
+  uint32_t k;             /* [k] winners per column */
+  uint32_t ktest;         /* [ktest] readout-only k override, 0 = k */
+  uint32_t dthr;          /* [dthr] dendritic branch threshold */
+  uint32_t boost;         /* [boost] supralinear NMDA bonus */
+  uint32_t mode;          /* [mode] 0 point, 1 supralinear, 2 two-layer */
+  uint32_t biasup;        /* [biasup] already resolved (1 = auto is resolved by the caller) */
+  uint32_t biasdown;      /* [biasdown] */
+  uint32_t biasshift;     /* [biasshift] */
+  uint32_t biasdownevery; /* [biasdownevery] */
+  uint32_t bandlo;        /* [bandlo] */
+  uint32_t bandhi;        /* [bandhi] */
+  uint32_t contrast;      /* [contrast] contrastive clamped/free phases */
+  uint32_t margingate;    /* [margingate] */
+  uint32_t hetero;        /* [hetero] */
+  uint32_t ltdrep;        /* [ltdrep] */
+  uint32_t ltdevery;      /* [ltdevery] >= 1 when contrast != 0 */
+  uint32_t facil;         /* [facil] readout-only facilitation */
+  uint32_t topkpar;       /* [topkpar] 1 = k_topk_par semantics, 0 = k_topk_serial */
+  uint32_t reserved[9];   /* zero */
+} axon_cfg;
+
+/* Fills `cfg` with the reference's built-in defaults (not config C). */
+void axon_cfg_defaults(axon_cfg* cfg);
+
+typedef struct axon_net axon_net;
+
+/* Device buffers of one network, named after the reference's MTLBuffers
+ * (src/axon.mm:749-768). Sizes in uint32 words for ncol columns, N = 32*ncol. */
+typedef enum axon_buf {
+  AXON_BUF_W0 = 0, AXON_BUF_W1 = 1, AXON_BUF_W2 = 2, AXON_BUF_W3 = 3, /* ncol*32*2*32*4 each */
+  AXON_BUF_CONN = 4,      /* ncol*32 : branch -> presynaptic group */
+  AXON_BUF_SPK_A = 5,     /* ncol : spike ballots, written on odd steps */
+  AXON_BUF_SPK_B = 6,     /* ncol : spike ballots, written on even steps */
+  AXON_BUF_DRIVE = 7,     /* ncol : column drive of the last step */
+  AXON_BUF_BBITS = 8,     /* N : branch-NMDA masks of the last step */
+  AXON_BUF_ACC = 9,       /* N : per-neuron drive of the last step */
+  AXON_BUF_BIAS = 10,     /* N : intrinsic bias */
+  AXON_BUF_MARG = 11,     /* ncol : k/(k+1) margin flag of the last step */
+  AXON_BUF_REFBALL = 12,  /* ncol : reference assembly whose members' drive is logged */
+  AXON_BUF_DRIVELOG = 13, /* 256 : 4 words per step (shared sum, count, exclusive sum, count) */
+  AXON_BUF_MULT = 14,     /* N : assembly multiplicity per neuron */
+  AXON_BUF_STIM = 15,     /* ncol : input clamp pattern of the last present */
+  AXON_BUF_STATS = 16,    /* 1024 : activity/plasticity counters of the last present */
+  AXON_BUF_HIST = 17,     /* 64*ncol : per-step spike ballots of the last present */
+  AXON_BUF_THETA = 18     /* 16 : [0] column threshold of the last step */
+} axon_buf;
+
+/* Allocates all device state of one network on `device` (0-based). Replaces the buffer
+ * allocation of src/axon.mm:749-768. */
+axon_status axon_create(const axon_cfg* cfg, int device, axon_net** out);
+axon_status axon_destroy(axon_net* net);
+
+/* Seeded weight-plane and connectivity init: k_init_w + k_init_conn, src/axon.mm:86-117,
+ * dispatched at src/axon.mm:770-781. Also zeroes bias, theta and stats. */
+axon_status axon_init(axon_net* net, uint32_t seed);
+
+/* One presentation: present(), src/axon.mm:815-888. `stim` is the ncol-word clamp
+ * pattern loadStim() builds (0 or 0xFFFFFFFF per input column). T steps in one
+ * persistent launch. use_bias: 0 off, 1 on, 2 = on while learning (the reference's
+ * default). Writes wall milliseconds per step to *ms_per_step when non-NULL. */
+axon_status axon_present(axon_net* net, const uint32_t* stim, uint32_t T, uint32_t clamp_steps,
+                         int learn, int freeze, uint32_t use_bias, double* ms_per_step);
+
+/* Copies a device buffer to / from host memory (`words` must equal the buffer size).
+ * Replaces the reference host's direct reads of shared MTLBuffer contents. */
+axon_status axon_read(axon_net* net, axon_buf which, uint32_t* host, uint64_t words);
+axon_status axon_write(axon_net* net, axon_buf which, const uint32_t* host, uint64_t words);
+uint64_t axon_buf_words(const axon_net* net, axon_buf which);
+
+/* Functional synapse count: k_wstat, src/axon.mm:641-646 (u32 wrap-around total). */
+axon_status axon_wstat(axon_net* net, uint32_t* count);
+
+/* Within-assembly functional density counters: k_within, src/axon.mm:524-562.
+ * out[10] (u32, added to by the call as the reference's atomics do; pass zeros).
+ * post_mask is read only when use_mask != 0 (N words); mult is N words or NULL (zeros). */
+axon_status axon_within(axon_net* net, const uint32_t* ball, uint32_t use_mask,
+                        const uint32_t* post_mask, const uint32_t* mult, uint32_t out[10]);
+
+/* Per-neuron functional in-degree over recurrent branches: k_indeg, src/axon.mm:566-581. */
+axon_status axon_indeg(axon_net* net, uint32_t* out_n);
+/* Per-neuron count of recurrent synapses still at 5 or 6: k_untouched, src/axon.mm:501-519. */
+axon_status axon_untouched(axon_net* net, uint32_t* out_n);
+/* Counter histogram: k_wdiag, src/axon.mm:591-638. memb N words, asm_spk nstim*ncol
+ * words, hist48 accumulated. */
+axon_status axon_wdiag(axon_net* net, const uint32_t* memb, const uint32_t* asm_spk,
+                       uint32_t nstim, uint32_t sel, uint32_t hist48[48]);
+/* Bit-serial known-answer hook: k_bstest, src/axon.mm:424-434. a0..a3 and m hold n
+ * words each (n a multiple of 4); op 0 inc, 1 dec, 2 clip [lo,hi]; planes updated. */
+axon_status axon_bstest(int device, uint32_t op, uint32_t lo, uint32_t hi, uint32_t* a0,
+                        uint32_t* a1, uint32_t* a2, uint32_t* a3, const uint32_t* m, uint64_t n);
+
+/* Stimulus patterns: `nstim` rows of `stimcols` input-column indices, drawn as
+ * src/axon.mm:793-799 does (mt19937(7 + seed*104729), libc++ shuffle of 0..incols-1). */
+axon_status axon_stimuli(uint32_t seed, uint32_t nstim, uint32_t incols, uint32_t stimcols, uint32_t* out);
+/* Clamp pattern of one presentation: loadStim, src/axon.mm:800-804. Keeps each of the
+ * `ncols` pattern columns with probability `keep` (mt19937(seed), tested in order). */
+axon_status axon_load_stim(const uint32_t* cols, uint32_t ncols, double keep, uint32_t seed, uint32_t ncol,
+                           uint32_t* out_ncol);
+
+/* Grid-wait limit of the persistent kernels in nanoseconds (default 2e9). */
+axon_status axon_set_wait_limit(axon_net* net, uint64_t ns);
+/* Text of the last error on this thread. */
+const char* axon_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AXON_CAPI_H */
