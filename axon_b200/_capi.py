@@ -31,6 +31,14 @@ class AxonCfg(C.Structure):
     _fields_ = [(f, C.c_uint32) for f in CFG_FIELDS] + [("reserved", C.c_uint32 * 9)]
 
 
+class RecallArgs(C.Structure):
+    _fields_ = [("T", C.c_uint32), ("clamp_steps", C.c_uint32), ("use_bias", C.c_uint32), ("method", C.c_uint32),
+                ("reserved", C.c_uint32 * 4)]
+
+
+RECALL_BATCHED, RECALL_PLAIN = 0, 1
+
+
 class AxonError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"axon status {status}: {msg}")
@@ -66,6 +74,11 @@ def lib() -> C.CDLL:
         L.axon_bstest.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, U32P, U32P, U32P, U32P, U32P,
                                   C.c_uint64]
         L.axon_set_wait_limit.argtypes = [C.c_void_p, C.c_uint64]
+        L.axon_stimuli.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, U32P]
+        L.axon_load_stim.argtypes = [U32P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, U32P]
+        for fn in (L.axon_recall, L.axon_recall_device):
+            fn.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(RecallArgs), C.c_void_p, C.c_void_p,
+                           C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
         _lib = L
     return _lib
 

@@ -158,4 +158,18 @@ axon_status axon_load_stim(const uint32_t* cols, uint32_t ncols, double keep, ui
   return AXON_OK;
 }
 
+axon_status axon_recall(axon_net* net, const uint32_t* cues, uint32_t B, const axon_recall_args* args,
+                        const uint32_t* ref_ball, uint32_t* final_spk, uint32_t* hist, uint32_t* stats,
+                        uint32_t* drive_log, double* gpu_ms) {
+  if (!net || !cues || !args) return fail(AXON_EINVAL, "null argument");
+  return net->recall(cues, B, *args, ref_ball, final_spk, hist, stats, drive_log, false, gpu_ms);
+}
+
+axon_status axon_recall_device(axon_net* net, const uint32_t* cues, uint32_t B, const axon_recall_args* args,
+                               const uint32_t* ref_ball, uint32_t* final_spk, uint32_t* hist, uint32_t* stats,
+                               uint32_t* drive_log, double* gpu_ms) {
+  if (!net || !cues || !args) return fail(AXON_EINVAL, "null argument");
+  return net->recall(cues, B, *args, ref_ball, final_spk, hist, stats, drive_log, true, gpu_ms);
+}
+
 }  // extern "C"

@@ -87,6 +87,7 @@ axon_status axon_net::create(const axon_cfg& c, int dev) {
   // launch shape: one column per warp when the grid fits in one wave, else 2 or 4
   cudaDeviceProp prop;
   CK(cudaGetDeviceProperties(&prop, device));
+  sm_count = prop.multiProcessorCount;
   shape.smem = present_smem_bytes(ncol, c.incols);
   bool ok = false;
   for (int cpw : {1, 2, 4}) {
@@ -110,6 +111,10 @@ axon_status axon_net::create(const axon_cfg& c, int dev) {
 }
 
 void axon_net::release() {
+  scratch.release();
+  io.release();
+  if (w3b) cudaFree(w3b);
+  w3b = nullptr;
   if (base) cudaFree(base);
   if (hstim) cudaFreeHost(hstim);
   if (hscratch) cudaFreeHost(hscratch);
@@ -128,6 +133,7 @@ axon_status axon_net::init(uint32_t seed) {
   CK(cudaMemsetAsync(d.stats, 0, 1024 * 4, stream));
   CK(cudaStreamSynchronize(stream));
   initialized = true;
+  w3b_valid = false;
   return AXON_OK;
 }
 
@@ -186,6 +192,7 @@ axon_status axon_net::present(const uint32_t* stim, uint32_t T, uint32_t clampSt
   CK(cudaMemsetAsync(d.stats, 0, 1024 * 4, stream));
   CK(cudaMemsetAsync(d.bar, 0, 4, stream));
   const PresentCfg pc = present_cfg(T, clampSteps, learn, useBias);
+  if (learn) w3b_valid = false;
   CK(cudaEventRecord(ev0, stream));
   CK(launch_present(d, pc, shape, stream));
   CK(cudaEventRecord(ev1, stream));
@@ -255,6 +262,7 @@ axon_status axon_net::write(axon_buf which, const uint32_t* host, uint64_t words
   CK(cudaMemcpyAsync(p, host, words * 4, cudaMemcpyHostToDevice, stream));
   CK(cudaStreamSynchronize(stream));
   if (which == AXON_BUF_W0 || which == AXON_BUF_CONN) initialized = true;
+  if (which == AXON_BUF_W3) w3b_valid = false;
   return AXON_OK;
 }
 

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/axon_capi.h"
+#include "batch.cuh"
 #include "plain.cuh"
 
 namespace axon {
@@ -17,6 +18,14 @@ axon_status set_error(axon_status s, const std::string& msg);
 std::string validate_cfg(const axon_cfg& c);
 
 }  // namespace axon
+
+// Grow-only device allocation reused across calls.
+struct DevArena {
+  void* p = nullptr;
+  size_t cap = 0;
+  axon_status ensure(size_t bytes);
+  void release();
+};
 
 struct axon_net {
   axon_cfg cfg{};
@@ -49,4 +58,13 @@ struct axon_net {
   axon_status wdiag(const uint32_t* memb, const uint32_t* asmSpk, uint32_t nstim, uint32_t sel, uint32_t hist48[48]);
   axon::PresentCfg present_cfg(uint32_t T, uint32_t clampSteps, bool learn, uint32_t useBias) const;
   axon_status check_device_error();
+
+  // batched readout
+  uint32_t* w3b = nullptr;      // W3 as [col][branch][word][lane], rebuilt when weights change
+  bool w3b_valid = false;
+  DevArena scratch, io;
+  int sm_count = 0;
+  axon_status recall(const uint32_t* cues, uint32_t B, const axon_recall_args& a, const uint32_t* refBall,
+                     uint32_t* finalOut, uint32_t* hist, uint32_t* stats, uint32_t* driveLog, bool dev, double* ms);
+  axon_status ensure_w3b();
 };

@@ -1,0 +1,185 @@
+// Host side of the batched readout (axon_recall / axon_recall_device).
+#include <algorithm>
+#include <cstring>
+
+#include "engine.hpp"
+
+using namespace axon;
+
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+
+axon_status DevArena::ensure(size_t bytes) {
+  if (bytes <= cap) return AXON_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  const size_t want = std::max(bytes, cap + cap / 2);
+  if (cudaMalloc(&p, want) != cudaSuccess) {
+    cudaGetLastError();
+    p = nullptr;
+    return set_error(AXON_ENOMEM, "device scratch allocation failed");
+  }
+  cap = want;
+  return AXON_OK;
+}
+
+void DevArena::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+}
+
+axon_status axon_net::ensure_w3b() {
+  if (w3b_valid) return AXON_OK;
+  if (!w3b) {
+    if (cudaMalloc(&w3b, plane_words * 4) != cudaSuccess) {
+      cudaGetLastError();
+      w3b = nullptr;
+      return set_error(AXON_ENOMEM, "W3 batch layout allocation failed");
+    }
+  }
+  CK(launch_make_w3b(d.W3, w3b, ncol, stream));
+  w3b_valid = true;
+  return AXON_OK;
+}
+
+namespace {
+size_t al(size_t bytes) { return (bytes + 255) & ~(size_t)255; }
+}  // namespace
+
+axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall_args& a, const uint32_t* refBall,
+                             uint32_t* finalOut, uint32_t* hist, uint32_t* stats, uint32_t* driveLog, bool dev,
+                             double* ms) {
+  if (!initialized) return set_error(AXON_ESTATE, "recall before init");
+  if (B == 0) return set_error(AXON_EINVAL, "B must be >= 1");
+  if (a.T == 0 || a.T > 64) return set_error(AXON_EINVAL, "T must be in 1..64");
+  if (a.use_bias > 1 || a.method > 1) return set_error(AXON_EINVAL, "bad use_bias or method");
+  CK(cudaSetDevice(device));
+
+  // ---- device views of the caller's arrays (copied in when they are host arrays)
+  const size_t bn = (size_t)B * ncol;
+  const uint32_t* dCues = cues;
+  const uint32_t* dRef = refBall;
+  uint32_t *dFinal = finalOut, *dHist = hist, *dStats = stats, *dLog = driveLog;
+  if (!dev) {
+    size_t need = al(bn * 4) + (refBall ? al(bn * 4) : 0) + (finalOut ? al(bn * 4) : 0) +
+                  (hist ? al(bn * a.T * 4) : 0) + (stats ? al((size_t)B * 4096) : 0) + (driveLog ? al((size_t)B * 1024) : 0);
+    axon_status st = io.ensure(need);
+    if (st != AXON_OK) return st;
+    char* p = (char*)io.p;
+    auto take = [&](size_t bytes) { uint32_t* r = (uint32_t*)p; p += al(bytes); return r; };
+    uint32_t* c = take(bn * 4);
+    CK(cudaMemcpyAsync(c, cues, bn * 4, cudaMemcpyHostToDevice, stream));
+    dCues = c;
+    if (refBall) {
+      uint32_t* r = take(bn * 4);
+      CK(cudaMemcpyAsync(r, refBall, bn * 4, cudaMemcpyHostToDevice, stream));
+      dRef = r;
+    }
+    if (finalOut) dFinal = take(bn * 4);
+    if (hist) dHist = take(bn * a.T * 4);
+    if (stats) dStats = take((size_t)B * 4096);
+    if (driveLog) {
+      dLog = take((size_t)B * 1024);
+      CK(cudaMemcpyAsync(dLog, driveLog, (size_t)B * 1024, cudaMemcpyHostToDevice, stream));
+    }
+  }
+  if (dStats) CK(cudaMemsetAsync(dStats, 0, (size_t)B * 4096, stream));
+
+  float gpu_ms = 0.f;
+  if (a.method == AXON_RECALL_PLAIN) {
+    // one persistent presentation launch per trajectory
+    const size_t zbytes = al(ncol * 4);
+    axon_status st = scratch.ensure(zbytes + al(1024 * 4));
+    if (st != AXON_OK) return st;
+    uint32_t* zeros = (uint32_t*)scratch.p;
+    uint32_t* statsTmp = (uint32_t*)((char*)scratch.p + zbytes);
+    CK(cudaMemsetAsync(zeros, 0, ncol * 4, stream));
+    const PresentCfg pc = present_cfg(a.T, a.clamp_steps, false, a.use_bias);
+    CK(cudaEventRecord(ev0, stream));
+    for (uint32_t b = 0; b < B; ++b) {
+      NetDev dd = d;
+      dd.stim = const_cast<uint32_t*>(dCues) + (size_t)b * ncol;
+      dd.refBall = dRef ? const_cast<uint32_t*>(dRef) + (size_t)b * ncol : zeros;
+      if (dHist) dd.hist = dHist + (size_t)b * a.T * ncol;
+      dd.stats = dStats ? dStats + (size_t)b * 1024 : statsTmp;
+      if (!dStats) CK(cudaMemsetAsync(statsTmp, 0, 1024 * 4, stream));
+      if (dLog) dd.driveLog = dLog + (size_t)b * 256;
+      dd.finalOut = dFinal ? dFinal + (size_t)b * ncol : nullptr;
+      CK(cudaMemsetAsync(d.bar, 0, 4, stream));
+      CK(launch_present(dd, pc, shape, stream));
+    }
+    CK(cudaEventRecord(ev1, stream));
+  } else {
+    axon_status st = ensure_w3b();
+    if (st != AXON_OK) return st;
+    const uint32_t ngrp = ncol / 8u, nactw = (((ngrp + 31u) / 32u) + 3u) & ~3u;
+    const PresentCfg pc = present_cfg(a.T, a.clamp_steps, false, a.use_bias);
+    RecallCfg rc{};
+    rc.ncol = ncol; rc.incols = cfg.incols; rc.B = B; rc.T = a.T; rc.clampSteps = a.clamp_steps;
+    rc.useBias = pc.useBias; rc.k = pc.k; rc.dthr = pc.dthr; rc.boost = pc.boost; rc.mode = pc.mode;
+    rc.targetCols = pc.targetCols; rc.facil = pc.facil; rc.biasShift = pc.biasShift; rc.topkPar = pc.topkPar;
+    rc.waitNs = wait_ns;
+    // per-neuron drive fits 16 bits unless branches can add more than 65535 in total
+    const uint64_t maxAcc = (cfg.mode == 2 ? 32ull : 32ull * (256ull + cfg.boost)) + cfg.facil;
+    rc.acc32 = maxAcc > 65535ull ? 1u : 0u;
+    uint32_t cpi = 1;
+    while (cpi < 32 && (uint64_t)cpi * 2 * B <= 32) cpi *= 2;
+    rc.cpi = cpi;
+    const size_t accBytes = bn * 32 * (rc.acc32 ? 4 : 2);
+    const size_t need = al(2 * bn * 4) + al(2ull * B * nactw * 4) + al(bn * 4) + al(accBytes) + al(64 * 4);
+    st = scratch.ensure(need);
+    if (st != AXON_OK) return st;
+    char* p = (char*)scratch.p;
+    auto take = [&](size_t bytes) { char* r = p; p += al(bytes); return r; };
+    RecallDev rd{};
+    rd.W3B = w3b;
+    rd.conn = d.conn;
+    rd.bias = d.bias;
+    rd.mult = d.mult;
+    rd.stims = dCues;
+    rd.refBall = dRef;
+    rd.spk = (uint32_t*)take(2 * bn * 4);
+    rd.act = (uint32_t*)take(2ull * B * nactw * 4);
+    rd.drv = (uint32_t*)take(bn * 4);
+    rd.acc = take(accBytes);
+    rd.work = (uint32_t*)take(64 * 4);
+    rd.finalOut = dFinal;
+    rd.hist = dHist;
+    rd.stats = dStats;
+    rd.driveLog = dLog;
+    rd.theta = nullptr;
+    rd.bar = d.bar;
+    rd.err = d.err;
+    CK(cudaMemsetAsync(rd.spk, 0, bn * 4, stream));
+    CK(cudaMemsetAsync(rd.act, 0, (size_t)B * nactw * 4, stream));
+    CK(cudaMemsetAsync(rd.work, 0, 64 * 4, stream));
+    CK(cudaMemsetAsync(d.bar, 0, 4, stream));
+    RecallShape rs{};
+    rs.threads = 1024;
+    rs.smem = recall_smem_bytes(ncol);
+    int per_sm = 0;
+    CK(recall_max_blocks_per_sm(rc.acc32, rs.threads, rs.smem, &per_sm));
+    if (per_sm < 1) return set_error(AXON_EINVAL, "batched recall kernel does not fit one SM");
+    rs.grid = sm_count * per_sm;
+    CK(cudaEventRecord(ev0, stream));
+    CK(launch_recall(rd, rc, rs, stream));
+    CK(cudaEventRecord(ev1, stream));
+  }
+  axon_status st = check_device_error();
+  if (st != AXON_OK) return st;
+  CK(cudaEventElapsedTime(&gpu_ms, ev0, ev1));
+  if (ms) *ms = gpu_ms;
+  if (!dev) {
+    if (finalOut) CK(cudaMemcpyAsync(finalOut, dFinal, bn * 4, cudaMemcpyDeviceToHost, stream));
+    if (hist) CK(cudaMemcpyAsync(hist, dHist, bn * a.T * 4, cudaMemcpyDeviceToHost, stream));
+    if (stats) CK(cudaMemcpyAsync(stats, dStats, (size_t)B * 4096, cudaMemcpyDeviceToHost, stream));
+    if (driveLog) CK(cudaMemcpyAsync(driveLog, dLog, (size_t)B * 1024, cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+  return AXON_OK;
+}

@@ -81,6 +81,48 @@ class Network:
         arr = np.ascontiguousarray(arr, dtype=np.uint32)
         A.check(A.lib().axon_write(self._h, A.BUF[name], A.u32(arr), arr.size))
 
+    def recall(self, cues: np.ndarray, T: int, clamp_steps: int, use_bias: int = 0, method: str = "batched",
+               hist: bool = False, stats: bool = False, ref_ball: np.ndarray | None = None,
+               drive_log: np.ndarray | None = None) -> dict:
+        """B readout trajectories (present() with learn=0 for each cue row) in one call.
+
+        Returns {"final": (B, ncol), "hist": (B, T, ncol) | None, "stats": (B, 1024) | None,
+        "drive_log": (B, 256) | None, "gpu_ms": float}.
+        """
+        cues = np.ascontiguousarray(cues, dtype=np.uint32)
+        B = cues.shape[0]
+        assert cues.shape == (B, self.ncol)
+        a = A.RecallArgs(T=T, clamp_steps=clamp_steps, use_bias=use_bias,
+                         method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN)
+        out = {"final": np.empty((B, self.ncol), dtype=np.uint32),
+               "hist": np.empty((B, T, self.ncol), dtype=np.uint32) if hist else None,
+               "stats": np.empty((B, 1024), dtype=np.uint32) if stats else None,
+               "drive_log": None}
+        rb = None
+        if ref_ball is not None:
+            rb = np.ascontiguousarray(ref_ball, dtype=np.uint32)
+            assert rb.shape == (B, self.ncol)
+        if drive_log is not None or rb is not None:
+            out["drive_log"] = (np.zeros((B, 256), dtype=np.uint32) if drive_log is None
+                                else np.ascontiguousarray(drive_log, dtype=np.uint32).copy())
+        ptr = lambda x: None if x is None else x.ctypes.data_as(C.c_void_p)  # noqa: E731
+        ms = C.c_double()
+        A.check(A.lib().axon_recall(self._h, ptr(cues), B, C.byref(a), ptr(rb), ptr(out["final"]), ptr(out["hist"]),
+                                    ptr(out["stats"]), ptr(out["drive_log"]), C.byref(ms)))
+        out["gpu_ms"] = ms.value
+        return out
+
+    def recall_device(self, cues_ptr: int, B: int, T: int, clamp_steps: int, final_ptr: int | None = None,
+                      use_bias: int = 0, method: str = "batched") -> float:
+        """Device-resident variant: cues/final are device addresses on this network's GPU."""
+        a = A.RecallArgs(T=T, clamp_steps=clamp_steps, use_bias=use_bias,
+                         method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN)
+        ms = C.c_double()
+        A.check(A.lib().axon_recall_device(self._h, C.c_void_p(cues_ptr), B, C.byref(a), None,
+                                           None if final_ptr is None else C.c_void_p(final_ptr), None, None, None,
+                                           C.byref(ms)))
+        return ms.value
+
     def final_spikes(self, T: int) -> np.ndarray:
         """The spike buffer present() wrote last (spkB after an odd T, spkA after an even T)."""
         return self.read("SPK_B" if (T & 1) else "SPK_A")

@@ -1,0 +1,363 @@
+"""Benchmark: batched recall on one trained AXON network, synaptic events/s on B200.
+
+Workload (the batched-recall configuration): config C network (131,072 neurons, 512 MiB of
+4-bit counters), 60 patterns, seed 0, trained for 40 epochs by the plain GPU path (setup,
+untimed). 300 cues = the 60 stored patterns plus noisy variants in which a fraction 0.1 or
+0.25 of each pattern's 64 columns is moved to other input columns (2 seeded draws each).
+Every trajectory is 10 clamped + 35 free steps with the intrinsic bias off (the reference's
+readout setting). One bench step = one batched recall of all 300 trajectories.
+
+Synaptic event: one presynaptic spike delivered to one postsynaptic neuron through conn,
+i.e. per step sum over (column, branch) of 32 * popcount(spikes of the branch's group at
+t-1). The count is fixed by the workload (identical for every method and for the oracle).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl axon|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+NCOL, INCOLS, STIMCOLS, LOAD, EPOCHS, SEED = 4096, 512, 64, 60, 40, 0
+T_RECALL, CLAMP_RECALL = 45, 10
+FLIPS = (0.10, 0.25)
+DRAWS = 2
+L2_BYTES = 126 * 2 ** 20
+
+
+def config_c():
+    import axon_b200 as ax
+
+    return ax.config(ncol=NCOL, incols=INCOLS, **ax.CONFIG_C)
+
+
+def noisy_cue(pattern: np.ndarray, frac: float, seed: int, rng_cls=np.random.default_rng) -> np.ndarray:
+    """Clamp words of a pattern with round(frac * len) of its columns moved to input
+    columns outside the pattern (seeded)."""
+    rng = rng_cls(seed)
+    n = len(pattern)
+    nflip = int(round(frac * n))
+    out_cols = rng.choice(n, nflip, replace=False)
+    others = np.setdiff1d(np.arange(INCOLS), pattern)
+    new = rng.choice(others, nflip, replace=False)
+    cols = pattern.copy()
+    cols[out_cols] = new
+    stim = np.zeros(NCOL, dtype=np.uint32)
+    stim[cols] = 0xFFFFFFFF
+    return stim
+
+
+def make_cues(pats: np.ndarray) -> np.ndarray:
+    cues = []
+    for q in range(LOAD):
+        stim = np.zeros(NCOL, dtype=np.uint32)
+        stim[pats[q]] = 0xFFFFFFFF
+        cues.append(stim)
+    for fi, f in enumerate(FLIPS):
+        for d in range(DRAWS):
+            for q in range(LOAD):
+                cues.append(noisy_cue(pats[q], f, 90000 + q * 16 + fi * 4 + d))
+    return np.stack(cues)
+
+
+def events_per_step(hist: np.ndarray, conn: np.ndarray) -> np.ndarray:
+    """Synaptic events of every (trajectory, step) from the spike history (B, T, ncol)."""
+    ngrp = NCOL // 8
+    fan = np.bincount(conn.astype(np.int64), minlength=ngrp).astype(np.float64)  # (col, branch) per group
+    pc = np.bitwise_count(hist).reshape(hist.shape[0], hist.shape[1], ngrp, 8).sum(-1, dtype=np.int64)
+    ev = np.zeros(hist.shape[:2], dtype=np.float64)
+    ev[:, 1:] = 32.0 * (pc[:, :-1] * fan).sum(-1)
+    return ev
+
+
+def train(net, pats) -> float:
+    import axon_b200 as ax
+
+    t0 = time.time()
+    for ep in range(EPOCHS):
+        for p in range(LOAD):
+            net.present(ax.load_stim(pats[p], 1.0, 1000 + p, NCOL), 10, 5, True)
+    net.present(ax.load_stim(pats[0], 1.0, 31337, NCOL), 10, 5, True)  # the reference's extra presentation
+    return time.time() - t0
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.rows.append([x.strip() for x in ln.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 2 + i and r[2 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_setup(gpus: int):
+    if gpus <= 1 or "RANK" not in os.environ:
+        return 0, 1, None
+    import torch
+    import torch.distributed as dist
+
+    rank, world = int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
+    from datetime import timedelta
+
+    dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    return rank, world, dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(x: float, dist) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_sample(cfg, gpu_net, cues, ev, threads: int, ntraj: int) -> dict:
+    """The CPU oracle on a bounded sample of the same trajectories (same trained state)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as O
+
+    cpu = O.OracleNet(cfg, threads=threads)
+    for name in ("W0", "W1", "W2", "W3", "CONN", "BIAS"):
+        cpu.write(name, gpu_net.read(name))
+    idx = np.linspace(0, cues.shape[0] - 1, ntraj).astype(int)
+    t0 = time.perf_counter()
+    for b in idx:
+        cpu.present(cues[b], T_RECALL, CLAMP_RECALL, False, True, 0)
+    dt = time.perf_counter() - t0
+    cpu.close()
+    return {"value": float(ev[idx].sum() / dt), "unit": "synaptic events/s", "cores": threads, "kind": "port",
+            "sample": f"{ntraj} of the 300 trajectories x {T_RECALL} steps, oracle present(learn=0), {dt:.1f} s"}
+
+
+def run_reference(args) -> None:
+    """Reference arm: the CPU restatement of the reference (oracle) on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as O
+
+    threads = os.cpu_count() or 1
+    cfg = config_c()
+    pats = O.stimuli(SEED, LOAD, INCOLS, STIMCOLS)
+    cues = make_cues(pats)
+    cpu = O.OracleNet(cfg, threads=threads)
+    cpu.init(SEED)
+    t0 = time.time()
+    for ep in range(EPOCHS):
+        for p in range(LOAD):
+            cpu.present(O.load_stim(pats[p], 1.0, 1000 + p, NCOL), 10, 5, True)
+    cpu.present(O.load_stim(pats[0], 1.0, 31337, NCOL), 10, 5, True)
+    train_s = time.time() - t0
+    conn = cpu.read("CONN")
+    ntraj = max(1, args.ref_traj)
+    idx = np.linspace(0, cues.shape[0] - 1, ntraj).astype(int)
+    times, evs = [], []
+    for it in range(args.warmup + args.steps):
+        ev = 0.0
+        t1 = time.perf_counter()
+        hists = []
+        for b in idx:
+            cpu.present(cues[b], T_RECALL, CLAMP_RECALL, False, True, 0)
+            hists.append(cpu.read("HIST")[: T_RECALL * NCOL].reshape(T_RECALL, NCOL))
+        dt = time.perf_counter() - t1
+        ev = events_per_step(np.stack(hists), conn).sum()
+        if it >= args.warmup:
+            times.append(dt)
+            evs.append(ev)
+    value = float(sum(evs) / sum(times))
+    line = {"impl": "reference", "metric": "synaptic events/s (batched recall, 300 trajectories x 45 steps)",
+            "value": value, "unit": "synaptic events/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded cues)",
+            "config": {"workload": "batched recall, config C load 60 seed 0, 300 cues x (10 clamp + 35 free)",
+                       "sample_trajectories": int(ntraj), "train_s": round(train_s, 1)},
+            "cpu_baseline": {"value": value, "unit": "synaptic events/s", "cores": threads, "kind": "port",
+                             "sample": f"{ntraj} trajectories x {T_RECALL} steps per step"},
+            "e2e": {"value": value, "unit": "synaptic events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="axon", choices=["axon", "reference"])
+    ap.add_argument("--ref-traj", type=int, default=6)
+    ap.add_argument("--cpu-traj", type=int, default=6)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    assert args.warmup >= 3, "at least 3 warm-up steps"
+    rank, world, dist = dist_setup(args.gpus)
+    import torch
+
+    import axon_b200 as ax
+    from axon_b200 import build
+
+    if rank == 0:
+        build.build_lib()
+    barrier(dist)
+    dev = torch.cuda.current_device()
+    cfg = config_c()
+    net = ax.Network(cfg, device=dev)
+    net.init(SEED)
+    pats = ax.stimuli(SEED, LOAD, INCOLS, STIMCOLS)
+    train_s = train(net, pats)
+    cues = make_cues(pats)
+    B = cues.shape[0]
+    # events of the workload (fixed by the trajectories), from one recorded run
+    ref = net.recall(cues, T_RECALL, CLAMP_RECALL, hist=True)
+    conn = net.read("CONN")
+    ev = events_per_step(ref["hist"], conn)
+    events = float(ev.sum())
+    active_tiles = None
+
+    # device-resident inputs and outputs
+    d_cues = torch.from_numpy(cues.view(np.int32)).to(f"cuda:{dev}")
+    d_final = torch.empty((B, NCOL), dtype=torch.int32, device=f"cuda:{dev}")
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=f"cuda:{dev}")
+    for _ in range(args.warmup):
+        net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_final.data_ptr())
+    assert np.array_equal(d_final.cpu().numpy().view(np.uint32), ref["final"])
+    times = []
+    torch.cuda.synchronize()
+    barrier(dist)
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            flush.zero_()  # evict L2 between timed steps (untimed: outside the device-timed launch)
+            torch.cuda.synchronize()
+            times.append(net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_final.data_ptr()))
+        torch.cuda.synchronize()
+    barrier(dist)
+    ms = max_over_ranks(float(np.mean(times)), dist)
+    value = world * events / (ms / 1e3)
+
+    # end to end through the public C-ABI call with pinned host buffers
+    h_cues = torch.from_numpy(cues.view(np.int32)).pin_memory().numpy().view(np.uint32)
+    e2e_t = []
+    for it in range(0 if args.no_e2e else args.warmup + max(3, args.steps // 2)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = net.recall(h_cues, T_RECALL, CLAMP_RECALL)
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            e2e_t.append(dt)
+    if e2e_t:
+        assert np.array_equal(r["final"], ref["final"])
+    e2e_s = max_over_ranks(float(np.mean(e2e_t)) if e2e_t else float("nan"), dist)
+
+    # plain GPU path on the same 300 trajectories (one persistent launch per trajectory)
+    plain = None
+    if not args.no_plain:
+        rp = net.recall(cues, T_RECALL, CLAMP_RECALL, method="plain")
+        assert np.array_equal(rp["final"], ref["final"])
+        pt = [net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_final.data_ptr(), method="plain")
+              for _ in range(2)]
+        pms = max_over_ranks(float(np.mean(pt)), dist)
+        plain = {"value": world * events / (pms / 1e3), "ms_per_step": pms, "launches_per_step": B}
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    hbm, peak_kind = peaks()
+    # roofline of the batched kernel: W3 (128 MiB, read once per recall step for all
+    # trajectories) + the per-neuron u16 drive slab written every step + spike vectors
+    w3_bytes = NCOL * 32 * 1024
+    slab = B * NCOL * 32 * 2
+    spikes = 2 * B * NCOL * 4
+    alg_bytes = T_RECALL * (w3_bytes + slab + spikes)
+    achieved = alg_bytes / (ms / 1e3) / 1e9
+    cpu = None if args.no_cpu else cpu_sample(cfg, net, cues, ev, os.cpu_count() or 1, args.cpu_traj)
+    line = {
+        "metric": "synaptic events/s (batched recall, 300 trajectories x 45 steps)",
+        "value": value, "unit": "synaptic events/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded cues from the reference's stimulus stream)",
+        "config": {"workload": "batched recall, config C load 60 seed 0, 300 cues x (10 clamp + 35 free), bias off",
+                   "trajectories": B, "steps_per_trajectory": T_RECALL, "events_per_batch": events,
+                   "train_s": round(train_s, 2), "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "note": "algorithmic bytes = 45 x (W3 128 MiB + u16 drive slab + spike vectors); the kernel is "
+                             "issue-bound, see profiles/"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * events / e2e_s, "unit": "synaptic events/s", "h2d_bytes_per_step": int(cues.nbytes),
+                "d2h_bytes_per_step": int(B * NCOL * 4)},
+        "plain": plain,
+        "batched_over_plain": (value / plain["value"]) if plain else None,
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

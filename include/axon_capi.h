@@ -138,6 +138,35 @@ axon_status axon_stimuli(uint32_t seed, uint32_t nstim, uint32_t incols, uint32_
 axon_status axon_load_stim(const uint32_t* cols, uint32_t ncols, double keep, uint32_t seed, uint32_t ncol,
                            uint32_t* out_ncol);
 
+/* ---------------------------------------------------------------- batched readout
+ * B readout trajectories of one network, each exactly what present() with learn = 0 does
+ * (src/axon.mm:815-888): `cues` holds B clamp patterns of ncol words. The batched method
+ * runs all B in one launch that reads each W3 tile once for every trajectory; the plain
+ * method runs them one presentation at a time (same results, for comparison). Outputs
+ * are optional (NULL to skip): final_spk B*ncol spikes of the last step, hist B*T*ncol
+ * spikes of every step, stats B*1024 counters of k_emit (word 2, the branch-coincidence
+ * count, is produced by the plain method only), drive_log B*256 added to like the
+ * reference's driveLog buffer for the members marked in ref_ball (B*ncol, NULL = none;
+ * the shared/exclusive split uses the network's MULT buffer). gpu_ms receives the
+ * device time of the launches. The network's per-present buffers are left undefined. */
+typedef enum axon_recall_method { AXON_RECALL_BATCHED = 0, AXON_RECALL_PLAIN = 1 } axon_recall_method;
+
+typedef struct axon_recall_args {
+  uint32_t T;           /* steps per trajectory, 1..64 */
+  uint32_t clamp_steps; /* leading steps clamped to the cue */
+  uint32_t use_bias;    /* 0 off (the reference's readout default), 1 on */
+  uint32_t method;      /* axon_recall_method */
+  uint32_t reserved[4]; /* zero */
+} axon_recall_args;
+
+axon_status axon_recall(axon_net* net, const uint32_t* cues, uint32_t B, const axon_recall_args* args,
+                        const uint32_t* ref_ball, uint32_t* final_spk, uint32_t* hist, uint32_t* stats,
+                        uint32_t* drive_log, double* gpu_ms);
+/* As axon_recall, with every array in device memory of the network's GPU (no copies). */
+axon_status axon_recall_device(axon_net* net, const uint32_t* cues, uint32_t B, const axon_recall_args* args,
+                               const uint32_t* ref_ball, uint32_t* final_spk, uint32_t* hist, uint32_t* stats,
+                               uint32_t* drive_log, double* gpu_ms);
+
 /* Grid-wait limit of the persistent kernels in nanoseconds (default 2e9). */
 axon_status axon_set_wait_limit(axon_net* net, uint64_t ns);
 /* Text of the last error on this thread. */

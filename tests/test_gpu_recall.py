@@ -1,0 +1,98 @@
+"""GPU parity of the batched readout: each of B trajectories of axon_recall equals the
+oracle's present(learn=0) for that cue (final spikes, every step's spikes, k_emit
+counters, member-drive log), for the batched and the plain method."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+
+def trained_pair(cfgkw, nstim, epochs, stimcols, seed=0):
+    import axon_b200 as ax
+
+    base = dict(ncol=256, incols=64, inbr=4, nand=4, target=16, k=12, dthr=1, mode=1, contrast=1, margingate=0,
+                ltdrep=1, ltdevery=2, biasup=73, biasdown=1)
+    base.update(cfgkw)
+    cfg = ax.config(**base)
+    gpu = ax.Network(cfg)
+    gpu.init(seed)
+    pats = ax.stimuli(seed, nstim, cfg.incols, stimcols)
+    for _ in range(epochs):
+        for p in range(nstim):
+            gpu.present(ax.load_stim(pats[p], 1.0, 1000 + p, cfg.ncol), 10, 5, True)
+    cpu = O.OracleNet(cfg)
+    for name in ("W0", "W1", "W2", "W3", "CONN", "BIAS"):
+        cpu.write(name, gpu.read(name))
+    return cfg, gpu, cpu, pats
+
+
+def make_cues(pats, ncol, B, rng):
+    import axon_b200 as ax
+
+    keeps = [1.0, 0.75, 0.5, 0.35, 0.25, 0.1, 0.0]
+    return np.stack([ax.load_stim(pats[b % len(pats)], keeps[b % len(keeps)], 4400 + b, ncol) for b in range(B)])
+
+
+def oracle_runs(cpu, cues, T, clamp, use_bias, ref=None):
+    finals, hists, stats, logs = [], [], [], []
+    for b in range(cues.shape[0]):
+        cpu.write("DRIVELOG", np.zeros(256, dtype=np.uint32))
+        cpu.write("REFBALL", ref[b] if ref is not None else np.zeros(cues.shape[1], dtype=np.uint32))
+        cpu.present(cues[b], T, clamp, False, True, use_bias)
+        finals.append(cpu.read("SPK_B" if T & 1 else "SPK_A"))
+        hists.append(cpu.read("HIST")[: T * cues.shape[1]].reshape(T, -1))
+        stats.append(cpu.read("STATS"))
+        logs.append(cpu.read("DRIVELOG"))
+    return np.stack(finals), np.stack(hists), np.stack(stats), np.stack(logs)
+
+
+@pytest.mark.parametrize("method", ["batched", "plain"])
+@pytest.mark.parametrize("B,T,clamp,use_bias", [(1, 10, 5, 0), (7, 10, 5, 1), (40, 35, 5, 0), (33, 45, 10, 0)])
+def test_recall_matches_oracle_small(method, B, T, clamp, use_bias):
+    cfg, gpu, cpu, pats = trained_pair({}, 6, 3, 16)
+    rng = np.random.default_rng(B)
+    cues = make_cues(pats, cfg.ncol, B, rng)
+    ref = np.stack([gpu.final_spikes(10)] * B)
+    mult = rng.integers(0, 3, cfg.ncol * 32).astype(np.uint32)
+    gpu.write("MULT", mult)
+    cpu.write("MULT", mult)
+    r = gpu.recall(cues, T, clamp, use_bias=use_bias, method=method, hist=True, stats=True, ref_ball=ref)
+    f, h, s, dl = oracle_runs(cpu, cues, T, clamp, use_bias, ref)
+    assert np.array_equal(r["final"], f)
+    assert np.array_equal(r["hist"], h)
+    if method == "batched":  # word 2 (branch coincidence) is produced by the plain method only
+        s = s.copy()
+        s[:, 2] = 0
+        r["stats"][:, 2] = 0
+    assert np.array_equal(r["stats"], s)
+    assert np.array_equal(r["drive_log"], dl)
+
+
+@pytest.mark.parametrize("variant", [dict(mode=0, dthr=2), dict(mode=2, dthr=0, boost=9), dict(ktest=5, facil=40),
+                                     dict(topkpar=0, target=0), dict(target=300), dict(boost=2000)])
+def test_recall_variants(variant):
+    cfg, gpu, cpu, pats = trained_pair(variant, 4, 2, 16)
+    cues = make_cues(pats, cfg.ncol, 9, np.random.default_rng(0))
+    r = gpu.recall(cues, 20, 5, hist=True)
+    f, h, _, _ = oracle_runs(cpu, cues, 20, 5, 0)
+    assert np.array_equal(r["final"], f)
+    assert np.array_equal(r["hist"], h)
+
+
+def test_recall_batched_equals_plain_full_geometry():
+    """Config C network at full size (131,072 neurons): batched and plain readouts of
+    60 cues agree word for word, and a sample of trajectories matches the oracle."""
+    import axon_b200 as ax
+
+    cfg, gpu, cpu, pats = trained_pair(dict(ncol=4096, incols=512, target=64, k=24), 12, 2, 64)
+    cues = make_cues(pats, cfg.ncol, 60, np.random.default_rng(1))
+    rb = gpu.recall(cues, 45, 10, hist=True)
+    rp = gpu.recall(cues, 45, 10, hist=True, method="plain")
+    assert np.array_equal(rb["final"], rp["final"])
+    assert np.array_equal(rb["hist"], rp["hist"])
+    idx = [0, 13, 59]
+    f, h, _, _ = oracle_runs(cpu, cues[idx], 45, 10, 0)
+    assert np.array_equal(rb["final"][idx], f)
+    assert np.array_equal(rb["hist"][idx], h)
