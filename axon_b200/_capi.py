@@ -38,6 +38,14 @@ class RecallArgs(C.Structure):
 
 RECALL_BATCHED, RECALL_PLAIN = 0, 1
 
+STATE_DEV_FIELDS = ["w0", "w1", "w2", "w3", "conn", "bias", "mult", "refball", "stim", "spk_a", "spk_b", "drive",
+                    "bbits", "acc", "marg", "drive_log", "stats", "hist", "theta"]
+
+
+class StateDev(C.Structure):
+    """Device pointers for axon_present_static (caller-owned buffers)."""
+    _fields_ = [(f, C.c_void_p) for f in STATE_DEV_FIELDS]
+
 
 class AxonError(RuntimeError):
     def __init__(self, status: int, msg: str):
@@ -76,6 +84,8 @@ def lib() -> C.CDLL:
         L.axon_set_wait_limit.argtypes = [C.c_void_p, C.c_uint64]
         L.axon_stimuli.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, U32P]
         L.axon_load_stim.argtypes = [U32P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, U32P]
+        L.axon_present_static.argtypes = [C.POINTER(AxonCfg), C.POINTER(StateDev), C.c_uint32, C.c_uint32, C.c_int,
+                                          C.c_uint32]
         for fn in (L.axon_recall, L.axon_recall_device):
             fn.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(RecallArgs), C.c_void_p, C.c_void_p,
                            C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]

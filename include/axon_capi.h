@@ -167,6 +167,27 @@ axon_status axon_recall_device(axon_net* net, const uint32_t* cues, uint32_t B, 
                                const uint32_t* ref_ball, uint32_t* final_spk, uint32_t* hist, uint32_t* stats,
                                uint32_t* drive_log, double* gpu_ms);
 
+/* ---------------------------------------------------------------- allocation-free present
+ * No counterpart in the reference. For hosts that must not allocate device memory during
+ * a call (their own caching allocator owns the device, or allocation is forbidden after
+ * start-up): the same presentation as axon_present, run on buffers the caller already
+ * owns, passed as device pointers with the sizes listed for axon_buf (plus stim: ncol
+ * words, the clamp pattern). Allocates nothing - no cudaMalloc/cudaFree, no library
+ * allocation: the kernel's only scratch is a fixed device array in the library sized for
+ * ncol <= 4096 (about 64 KiB per GPU, held until the process exits); larger ncol returns
+ * AXON_EINVAL. Runs on the default stream and returns when the presentation is done.
+ * The first call on a device resolves the array's device address; make it before any
+ * stream capture. Calls that overlap on the GPU share that array and race: issue one at
+ * a time per device. */
+typedef struct axon_state_dev {
+  uint32_t *w0, *w1, *w2, *w3;                   /* bitplanes (in/out) */
+  uint32_t *conn, *bias, *mult, *refball, *stim; /* conn, mult, refball, stim in; bias in/out */
+  uint32_t *spk_a, *spk_b, *drive, *bbits, *acc, *marg, *drive_log, *stats, *hist, *theta; /* out */
+} axon_state_dev;
+
+axon_status axon_present_static(const axon_cfg* cfg, const axon_state_dev* state, uint32_t T,
+                                uint32_t clamp_steps, int learn, uint32_t use_bias);
+
 /* Grid-wait limit of the persistent kernels in nanoseconds (default 2e9). */
 axon_status axon_set_wait_limit(axon_net* net, uint64_t ns);
 /* Text of the last error on this thread. */
