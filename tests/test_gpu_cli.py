@@ -1,0 +1,69 @@
+"""The `axon` command line against the oracle's: identical stdout, line for line, apart
+from the banner's hardware name and wall-clock timings; and the published spot-check row
+scraped exactly as the reference's bench/cap10.sh scrapes it."""
+import json
+import subprocess
+from pathlib import Path
+
+import pytest
+
+import oracle_lib as O
+from metrics import scrape
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parents[1]
+GOLD = json.loads((Path(__file__).parent / "golden" / "published.json").read_text())
+CONFIG_C = GOLD["config_c"].split()
+SMALL = ["ncol=512", "incols=64", "stimcols=16", "target=24"]
+
+
+def engine_cli(args):
+    from axon_b200 import build
+
+    build.build_lib()
+    exe = build.build_cli()
+    p = subprocess.run([str(exe), *args], capture_output=True, text=True, timeout=1800)
+    assert p.returncode == 0, p.stderr
+    return p.stdout
+
+
+def comparable(out: str) -> list[str]:
+    keep = []
+    for ln in out.splitlines():
+        if ln.startswith(" AXON v0  -  columnar assembly engine"):
+            continue
+        if "ms/timestep" in ln or " st/s " in ln or "full step: serial" in ln:
+            continue
+        keep.append(ln)
+    return keep
+
+
+def assert_same(args):
+    a, b = comparable(engine_cli(args)), comparable(O.run_cli(args))
+    for i, (x, y) in enumerate(zip(a, b)):
+        assert x == y, f"line {i}:\n engine: {x}\n oracle: {y}"
+    assert len(a) == len(b)
+
+
+@pytest.mark.parametrize("extra", [
+    [*CONFIG_C, "stim=6", "epochs=3", "deep=1", "wave=1", "wavet=35", "split=1", "unionchar=1", "diag=1"],
+    [*CONFIG_C, "stim=5", "epochs=2", "vbs=1", "vtopk=1", "ktest=8", "facil=3", "quiet=1"],
+    ["stim=4", "epochs=2", "deep=1", "wave=1"],                      # the reference's built-in defaults
+    [*CONFIG_C, "stim=3", "epochs=0", "deep=1", "margingate=1", "hetero=1", "seed=9"],
+    [*CONFIG_C, "stim=7", "epochs=1", "T=20", "clampsteps=8", "trainclamp=6", "mode=0", "dthr=3", "wave=1",
+     "wavet=60", "biasdownevery=3"],
+])
+def test_cli_matches_oracle_small(extra):
+    assert_same([*SMALL, *extra])
+
+
+def test_cli_spot_check_full_size():
+    args = [*CONFIG_C, "stim=12", "epochs=40", "deep=1", "wave=1", "wavet=35"]
+    out = engine_cli(args)
+    m = scrape(out)
+    g = GOLD["spot_check"]
+    assert (m["within_pct"], m["recall"], m["best_other"], m["sustained"], m["drive_t6"]) == (
+        g["within_pct"], g["recall"], g["best_other"], g["sustained"], g["drive_t6"])
+    ref = comparable(O.run_cli(args))
+    assert comparable(out) == ref
