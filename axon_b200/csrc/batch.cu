@@ -2,21 +2,21 @@
 //
 // Readout presentations of rakib-nyc/axon (present() with learn=false, src/axon.mm:815-888)
 // change no weight, so any number of them can run together. One cooperative launch runs
-// T steps for all B trajectories, two grid barriers per step:
+// T steps for all B trajectories, two grid barriers per step.
 //
-//   phase 1  work items are columns (dynamically claimed). For its column, a warp per
-//            trajectory computes every neuron's drive over the branches whose presynaptic
-//            group is active in that trajectory: the warp gathers the spike words of up to
-//            four active branches in one coalesced load, ballots which are nonzero, and
-//            pops AND-counts only for nonzero words against W3 words that all B
-//            trajectories of the item read through L1. Per-neuron drive goes to a u16 (or
-//            u32) slab, the column drive to a [B][ncol] table.
-//   phase 2  per trajectory: the column threshold (block_theta), then the exact k-of-32
-//            ballot only for columns that pass the gate - a few dozen of 4096 - from the
-//            stored per-neuron drives; the new spike vector and its group-activity bits.
-//
-// W3 is re-laid out once per trained network as [col][branch][word][lane] so that a
-// warp's 32 lanes read one word of a tile from 128 contiguous bytes.
+//   phase 2 (end of step t-1) publishes, for every presynaptic group g, the list of
+//            trajectories in which g spiked, each entry carrying that trajectory's nonzero
+//            spike words of g (one 16-byte record; most groups have one or two).
+//   phase 1  work items are pairs of columns, claimed dynamically. The item's 64 W3 tiles
+//            (64 KiB, laid out [branch][row][word]) arrive by bulk TMA copies into shared
+//            memory, double-buffered so the next item loads while this one computes. The
+//            item's (branch, entry) pairs are flattened and dealt 32 per warp, one per lane:
+//            a lane pops AND-counts of its entry's words against all 32 rows of the tile
+//            and adds the dendritic terms into per-(trajectory, neuron) counters in shared
+//            memory (two 16-bit sums per 32-bit atomic). Silent (branch, trajectory) pairs
+//            cost nothing. The counters then become the per-neuron and column drives.
+//   phase 2  per trajectory: the column threshold (block_theta), the exact k-of-32 ballot
+//            only for columns that pass the gate, the new spike vector, and its group lists.
 #include <cstdint>
 
 #include "axon_device.cuh"
@@ -25,25 +25,58 @@
 
 namespace axon {
 
-__global__ void k_make_w3b(const uint4* __restrict__ W3, uint32_t* __restrict__ W3B, uint64_t ntile) {
-  // one thread per (tile, lane): reads 2 uint4, writes 8 words strided by 32
+__global__ void k_make_w3r(const uint4* __restrict__ W3, uint32_t* __restrict__ W3R, uint64_t ntile) {
+  // one thread per (tile, row): the row's two uint4 halves become 8 consecutive words
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ntile * 32) return;
   const uint64_t tile = i >> 5;
-  const uint32_t lane = (uint32_t)(i & 31u);
-  const uint4 a = W3[tile * kTileU4 + lane], b = W3[tile * kTileU4 + 32 + lane];
-  uint32_t* o = W3B + tile * 256 + lane;
-  o[0 * 32] = a.x; o[1 * 32] = a.y; o[2 * 32] = a.z; o[3 * 32] = a.w;
-  o[4 * 32] = b.x; o[5 * 32] = b.y; o[6 * 32] = b.z; o[7 * 32] = b.w;
+  const uint32_t row = (uint32_t)(i & 31u);
+  uint4* o = reinterpret_cast<uint4*>(W3R + tile * 256 + row * 8);
+  o[0] = W3[tile * kTileU4 + row];
+  o[1] = W3[tile * kTileU4 + 32 + row];
 }
 
-cudaError_t launch_make_w3b(const uint4* W3, uint32_t* W3B, uint32_t ncol, cudaStream_t st) {
+cudaError_t launch_make_w3r(const uint4* W3, uint32_t* W3R, uint32_t ncol, cudaStream_t st) {
   const uint64_t ntile = (uint64_t)ncol * kNslot;
-  k_make_w3b<<<(unsigned)((ntile * 32 + 255) / 256), 256, 0, st>>>(W3, W3B, ntile);
+  k_make_w3r<<<(unsigned)((ntile * 32 + 255) / 256), 256, 0, st>>>(W3, W3R, ntile);
   return cudaGetLastError();
 }
 
-// dendritic nonlinearity of k_drive, src/axon.mm:174-178
+// ---------------------------------------------------------------- TMA bulk copy + mbarrier
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// bounded wait for one phase of an mbarrier
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+  if (mbar_test(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_test(bar, parity)) return true;
+    if ((it & 255u) == 0u && globaltimer_ns() - t0 > limit_ns) return false;
+  }
+}
+
+// dendritic nonlinearity of k_drive, src/axon.mm:174-178 (applied to non-silent branches)
 __device__ __forceinline__ uint32_t branch_term(uint32_t cnt, const RecallCfg& c) {
   const bool nmda = cnt >= c.dthr;
   if (c.mode == 0u) return cnt;
@@ -51,86 +84,180 @@ __device__ __forceinline__ uint32_t branch_term(uint32_t cnt, const RecallCfg& c
   return nmda ? 1u : 0u;
 }
 
-template <typename AccT>
+constexpr uint32_t kColWords = kNslot * 256;           // one column's 32 tiles, [branch][row][word]
+constexpr uint32_t kItemWords = kRecallCpi * kColWords;  // one work item
+
+template <bool PACK>
 __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
-  extern __shared__ __align__(16) uint32_t sm[];
-  const uint32_t ncol = c.ncol, incols = c.incols, B = c.B;
-  const uint32_t ngrp = ncol / 8u, nactw = (((ngrp + 31u) / 32u) + 3u) & ~3u;
-  uint32_t* sD = sm;               // drives of one trajectory
-  uint32_t* sSpk = sD + ncol;      // its new spike vector
-  uint32_t* sList = sSpk + ncol;   // columns that need the k-of-32 ballot
-  uint32_t* sHist = sList + ncol;  // 256
-  uint32_t* sRed = sHist + 256;    // 96
-  uint32_t* sMisc = sRed + 96;     // [0] barrier flag, [1] work item, [2] list length
+  extern __shared__ __align__(128) uint32_t sm[];
+  const uint32_t ncol = c.ncol, incols = c.incols, B = c.B, ngrp = ncol / 8u;
+  constexpr uint32_t accStride = PACK ? 17u : 33u;  // padded: distinct trajectories hit distinct banks
+  uint32_t* sTile = sm;                                  // [2][kItemWords]
+  uint32_t* sAcc = sTile + 2 * kItemWords;               // [kRecallCpi][B][accStride]
+  uint32_t* sConn = sAcc + kRecallCpi * B * accStride;   // [64]
+  uint32_t* sP = sConn + 64;                             // [68] entry prefix over the item's 64 branches
+  uint32_t* sMisc = sP + 68;                             // [16]
+  uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
+  // phase-2 views reuse the tile buffers
+  uint32_t* sD = sTile;
+  uint32_t* sSpk = sTile + ncol;
+  uint32_t* sList = sTile + 2 * ncol;
+  uint32_t* sHist = sTile + 3 * ncol;
+  uint32_t* sRed = sHist + 256;
 
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
-  const uint32_t cpi = c.cpi, nitems = (ncol + cpi - 1) / cpi;
-  const uint32_t wsub = warp % cpi, bstart = warp / cpi, bstep = nw / cpi;
-  AccT* accv = reinterpret_cast<AccT*>(d.acc);
+  const uint32_t nitems = (ncol + kRecallCpi - 1) / kRecallCpi;
+  if (tid == 0) {
+    mbar_init(&sBar[0], 1);
+    mbar_init(&sBar[1], 1);
+    fence_proxy_async_smem();
+  }
+  __syncthreads();
+  uint32_t uses0 = 0, uses1 = 0;  // completed phases per buffer
+  uint32_t kbuf = 0;              // buffer of the next item
   uint32_t epoch = 0;
+
+  auto issue = [&](uint32_t item, uint32_t buf) {  // thread 0 only
+    const uint32_t c0 = item * kRecallCpi;
+    const uint32_t ncols = min(kRecallCpi, ncol - c0);
+    const uint32_t bytes = ncols * kColWords * 4u;
+    fence_proxy_async_smem();
+    mbar_expect_tx(&sBar[buf], bytes);
+    for (uint32_t k = 0; k < ncols; ++k)
+      bulk_g2s(sTile + buf * kItemWords + k * kColWords, d.W3R + (size_t)(c0 + k) * kColWords, kColWords * 4u, &sBar[buf]);
+  };
 
   for (uint32_t t = 0; t < c.T; ++t) {
     const uint32_t par = t & 1u;
     const uint32_t* spkIn = d.spk + (size_t)par * B * ncol;
     uint32_t* spkOut = d.spk + (size_t)(par ^ 1u) * B * ncol;
-    const uint32_t* actIn = d.act + (size_t)par * B * nactw;
-    uint32_t* actOut = d.act + (size_t)(par ^ 1u) * B * nactw;
+    const uint4* entIn = d.ent + (size_t)par * ngrp * B;
+    uint4* entOut = d.ent + (size_t)(par ^ 1u) * ngrp * B;
+    const uint32_t* cntIn = d.ecnt + par * ngrp;
+    uint32_t* cntOut = d.ecnt + (par ^ 1u) * ngrp;
     const bool clamp = t < c.clampSteps;
 
-    // ---------------- phase 1: drives of every (column, trajectory)
-    for (;;) {
-      if (tid == 0) sMisc[1] = atomicAdd(d.work + t, 1u);
+    // next step's list lengths start at zero (last read in phase 1 of step t-1)
+    if (blockIdx.x == 0)
+      for (uint32_t g = tid; g < ngrp; g += blockDim.x) cntOut[g] = 0u;
+
+    // ---------------- phase 1
+    if (tid == 0) {
+      const uint32_t it0 = atomicAdd(d.work + t, 1u);
+      sMisc[1] = it0;
+      if (it0 < nitems) issue(it0, kbuf);
+    }
+    __syncthreads();
+    uint32_t item = sMisc[1];
+    while (item < nitems) {
+      const uint32_t bcur = kbuf;
+      if (tid == 0) {
+        const uint32_t nx = atomicAdd(d.work + t, 1u);
+        sMisc[2] = nx;
+        sMisc[3] = 0u;
+        if (nx < nitems) issue(nx, bcur ^ 1u);
+      }
+      const uint32_t c0 = item * kRecallCpi;
+      for (uint32_t i = tid; i < 64u; i += blockDim.x) {
+        const uint32_t col = c0 + (i >> 5);
+        sConn[i] = col < ncol ? __ldg(d.conn + col * kNslot + (i & 31u)) : 0u;
+      }
+      for (uint32_t i = tid; i < kRecallCpi * B * accStride; i += blockDim.x) sAcc[i] = 0u;
       __syncthreads();
-      const uint32_t item = sMisc[1];
-      __syncthreads();
-      if (item >= nitems) break;
-      const uint32_t cc = item * cpi + wsub;
-      if (cc >= ncol || bstart >= B) continue;
-      const uint32_t gS = __ldg(d.conn + cc * kNslot + lane);  // lane = branch
-      const uint32_t biasL = c.useBias ? (__ldg(d.bias + cc * 32u + lane) >> c.biasShift) : 0u;
-      const bool logCol = d.refBall != nullptr && cc >= incols;
-      const uint32_t multL = logCol ? __ldg(d.mult + cc * 32u + lane) : 0u;
-      const uint32_t* wcol = d.W3B + (size_t)cc * (kNslot * 256u) + lane;
-      for (uint32_t b = bstart; b < B; b += bstep) {
-        const uint32_t* inb = spkIn + (size_t)b * ncol;
-        const uint32_t aw = __ldcg(actIn + (size_t)b * nactw + (gS >> 5));
-        uint32_t amask = __ballot_sync(kFull, (aw >> (gS & 31u)) & 1u);
-        uint32_t a = 0;
-        while (amask) {
-          uint32_t s4[4];
+      if (warp == 0) {  // prefix of the 64 list lengths
+        const bool v0 = c0 < ncol, v1 = c0 + 1 < ncol;
+        const uint32_t n0 = v0 ? __ldcg(cntIn + sConn[lane]) : 0u, n1 = v1 ? __ldcg(cntIn + sConn[32 + lane]) : 0u;
+        uint32_t i0 = n0, i1 = n1;
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            s4[u] = amask ? (uint32_t)(__ffs(amask) - 1) : 32u;
-            amask &= amask - 1u;
+        for (int off = 1; off < 32; off <<= 1) {
+          const uint32_t a = __shfl_up_sync(kFull, i0, off), b = __shfl_up_sync(kFull, i1, off);
+          if (lane >= (uint32_t)off) { i0 += a; i1 += b; }
+        }
+        const uint32_t tot0 = __shfl_sync(kFull, i0, 31);
+        sP[1 + lane] = i0;
+        sP[33 + lane] = tot0 + i1;
+        if (lane == 0) sP[0] = 0u;
+      }
+      const bool ok = mbar_wait(&sBar[bcur], (bcur ? uses1 : uses0) & 1u, c.waitNs);
+      if (bcur) ++uses1; else ++uses0;
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) atomicCAS(d.err, 0u, kErrTimeout);
+        mbar_wait(&sBar[bcur ^ 1u], (bcur ? uses0 : uses1) & 1u, c.waitNs);  // copies still in flight
+        return;
+      }
+      const uint32_t E = sP[64], units = (E + 31u) >> 5;
+      const uint32_t* tileBase = sTile + bcur * kItemWords;
+      for (;;) {
+        uint32_t u = 0;
+        if (lane == 0) u = atomicAdd(sMisc + 3, 1u);
+        u = __shfl_sync(kFull, u, 0);
+        if (u >= units) break;
+        const uint32_t flat = u * 32u + lane;
+        if (flat >= E) continue;
+        uint32_t sp = 0;
+#pragma unroll
+        for (uint32_t step = 32; step; step >>= 1)
+          if (sp + step < 64u && sP[sp + step] <= flat) sp += step;
+        const uint32_t e = flat - sP[sp];
+        const uint32_t g = sConn[sp];
+        const uint4 en = __ldcg(entIn + (size_t)g * B + e);
+        const uint32_t b = en.x & 0xFFFFu, nz = (en.x >> 16) & 0xFFu;
+        const uint32_t* tile = tileBase + (sp >> 5) * kColWords + (sp & 31u) * 256u;
+        uint32_t* accb = sAcc + ((sp >> 5) * B + b) * accStride;
+        const uint32_t w0 = (uint32_t)__ffs(nz) - 1u;
+        const uint32_t nz1 = nz & (nz - 1u);
+        const uint32_t nz2 = nz1 & (nz1 - 1u);
+        if (nz2 == 0u) {  // one or two nonzero words: the common case
+          const uint32_t w1 = nz1 ? (uint32_t)__ffs(nz1) - 1u : w0;
+          const uint32_t S0 = en.y, S1 = nz1 ? en.z : 0u;
+#pragma unroll 4
+          for (uint32_t r = 0; r < 32u; r += 2) {
+            const uint32_t* ra = tile + r * 8u;
+            const uint32_t q0 = __popc(ra[w0] & S0) + __popc(ra[w1] & S1);
+            const uint32_t q1 = __popc(ra[8 + w0] & S0) + __popc(ra[8 + w1] & S1);
+            const uint32_t t0 = branch_term(q0, c), t1 = branch_term(q1, c);
+            if (PACK) atomicAdd(accb + (r >> 1), t0 | (t1 << 16));
+            else { atomicAdd(accb + r, t0); atomicAdd(accb + r + 1, t1); }
           }
-          const uint32_t slot = lane >> 3, wd = lane & 7u;
-          const uint32_t mys = slot == 0 ? s4[0] : slot == 1 ? s4[1] : slot == 2 ? s4[2] : s4[3];
-          const uint32_t g = __shfl_sync(kFull, gS, mys & 31u);
-          const uint32_t word = mys < 32u ? __ldcg(inb + 8u * g + wd) : 0u;
-          const uint32_t nz = __ballot_sync(kFull, word != 0u);
+        } else {  // three or more nonzero words: counts in registers, words past the third from the spikes
+          uint32_t cnt[32];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            if (s4[u] >= 32u) break;
-            uint32_t m = (nz >> (8 * u)) & 0xFFu, cnt = 0;
-            const uint32_t* wt = wcol + s4[u] * 256u;
-            while (m) {
-              const uint32_t w2 = (uint32_t)(__ffs(m) - 1);
-              m &= m - 1u;
-              const uint32_t S = __shfl_sync(kFull, word, 8u * u + w2);
-              cnt += __popc(__ldg(wt + w2 * 32u) & S);
-            }
-            a += branch_term(cnt, c);
+          for (int r = 0; r < 32; ++r) cnt[r] = 0u;
+          uint32_t m = nz, k = 0;
+          while (m) {
+            const uint32_t w = (uint32_t)__ffs(m) - 1u;
+            m &= m - 1u;
+            const uint32_t S = k == 0 ? en.y : k == 1 ? en.z : k == 2 ? en.w : __ldcg(spkIn + (size_t)b * ncol + 8u * g + w);
+            ++k;
+#pragma unroll
+            for (int r = 0; r < 32; ++r) cnt[r] += __popc(tile[r * 8 + w] & S);
+          }
+#pragma unroll
+          for (int r = 0; r < 32; r += 2) {
+            const uint32_t t0 = branch_term(cnt[r], c), t1 = branch_term(cnt[r + 1], c);
+            if (PACK) atomicAdd(accb + (r >> 1), t0 | (t1 << 16));
+            else { atomicAdd(accb + r, t0); atomicAdd(accb + r + 1, t1); }
           }
         }
-        if (c.facil != 0u && ((__ldcg(inb + cc) >> lane) & 1u)) a += c.facil;
+      }
+      __syncthreads();
+      // per-neuron and column drives of the item's columns for every trajectory
+      for (uint32_t pp = warp; pp < kRecallCpi * B; pp += nw) {
+        const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
+        if (col >= ncol) continue;
+        const uint32_t* ab = sAcc + (colL * B + b) * accStride;
+        uint32_t a = PACK ? ((ab[lane >> 1] >> (16u * (lane & 1u))) & 0xFFFFu) : ab[lane];
+        if (c.facil != 0u && ((__ldcg(spkIn + (size_t)b * ncol + col) >> lane) & 1u)) a += c.facil;
+        const uint32_t biasL = c.useBias ? (__ldg(d.bias + col * 32u + lane) >> c.biasShift) : 0u;
         a = a > biasL ? a - biasL : 0u;
-        accv[((size_t)b * ncol + cc) * 32u + lane] = (AccT)a;
+        if (c.acc32) reinterpret_cast<uint32_t*>(d.acc)[((size_t)b * ncol + col) * 32u + lane] = a;
+        else reinterpret_cast<uint16_t*>(d.acc)[((size_t)b * ncol + col) * 32u + lane] = (uint16_t)a;
         const uint32_t dsum = __reduce_add_sync(kFull, a);
-        if (lane == 0) __stcg(d.drv + (size_t)b * ncol + cc, dsum);
-        if (logCol) {  // driveLog of k_emit, src/axon.mm:216-220
-          const uint32_t rb = __ldg(d.refBall + (size_t)b * ncol + cc);
+        if (lane == 0) __stcg(d.drv + (size_t)b * ncol + col, dsum);
+        if (d.refBall != nullptr && col >= incols) {  // driveLog of k_emit, src/axon.mm:216-220
+          const uint32_t rb = __ldg(d.refBall + (size_t)b * ncol + col);
           if (rb) {
-            const bool member = (rb >> lane) & 1u, shared = multL > 1u;
+            const bool member = (rb >> lane) & 1u, shared = __ldg(d.mult + col * 32u + lane) > 1u;
             const uint32_t mS = __ballot_sync(kFull, member && shared), mE = __ballot_sync(kFull, member && !shared);
             const uint32_t sumS = __reduce_add_sync(kFull, (member && shared) ? a : 0u);
             const uint32_t sumE = __reduce_add_sync(kFull, (member && !shared) ? a : 0u);
@@ -142,15 +269,18 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
           }
         }
       }
+      __syncthreads();
+      item = sMisc[2];
+      kbuf ^= 1u;
     }
     if (!grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;
 
-    // ---------------- phase 2: threshold, gated k-of-32 ballots, next spike vectors
+    // ---------------- phase 2: threshold, gated k-of-32 ballots, next spike vectors and lists
     for (uint32_t b = blockIdx.x; b < B; b += gridDim.x) {
       const uint32_t* drvb = d.drv + (size_t)b * ncol;
       for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x)
         reinterpret_cast<uint4*>(sD)[i] = __ldcg(reinterpret_cast<const uint4*>(drvb) + i);
-      if (tid == 0) sMisc[2] = 0u;
+      if (tid == 0) sMisc[4] = 0u;
       __syncthreads();
       const uint32_t theta = block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed);
       const uint32_t gate = max(theta, 1u);
@@ -158,14 +288,15 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
       for (uint32_t cc = tid; cc < ncol; cc += blockDim.x) {
         uint32_t v = 0u;
         if (clamp && cc < incols) v = __ldg(stimb + cc);
-        else if (sD[cc] >= gate) sList[atomicAdd(sMisc + 2, 1u)] = cc;
+        else if (sD[cc] >= gate) sList[atomicAdd(sMisc + 4, 1u)] = cc;
         sSpk[cc] = v;
       }
       __syncthreads();
-      const uint32_t npend = sMisc[2];
+      const uint32_t npend = sMisc[4];
       for (uint32_t e = warp; e < npend; e += nw) {
         const uint32_t cc = sList[e];
-        const uint32_t a = (uint32_t)__ldcg(accv + ((size_t)b * ncol + cc) * 32u + lane);
+        const uint32_t a = c.acc32 ? __ldcg(reinterpret_cast<const uint32_t*>(d.acc) + ((size_t)b * ncol + cc) * 32u + lane)
+                                   : (uint32_t)__ldcg(reinterpret_cast<const uint16_t*>(d.acc) + ((size_t)b * ncol + cc) * 32u + lane);
         uint32_t vk, vk1;
         const uint32_t ball = warp_kwta(a, lane, c.k, vk, vk1);
         if (lane == 0) {
@@ -191,15 +322,25 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
         if (d.hist) reinterpret_cast<uint4*>(d.hist + ((size_t)b * c.T + t) * ncol)[i] = v;
         if (d.finalOut && t + 1u == c.T) reinterpret_cast<uint4*>(d.finalOut + (size_t)b * ncol)[i] = v;
       }
-      for (uint32_t gb = warp * 32u; gb < nactw * 32u; gb += nw * 32u) {
-        const uint32_t g = gb + lane;
-        bool any = false;
-        if (g < ngrp) {
+      if (t + 1u < c.T) {  // group lists for the next step
+        for (uint32_t g = tid; g < ngrp; g += blockDim.x) {
           const uint4 p = reinterpret_cast<const uint4*>(sSpk)[2 * g], q = reinterpret_cast<const uint4*>(sSpk)[2 * g + 1];
-          any = (p.x | p.y | p.z | p.w | q.x | q.y | q.z | q.w) != 0u;
+          const uint32_t w[8] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w};
+          uint32_t nz = 0, S0 = 0u, S1 = 0u, S2 = 0u, k = 0;
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+            if (w[i]) {
+              nz |= 1u << i;
+              if (k == 0) S0 = w[i];
+              else if (k == 1) S1 = w[i];
+              else if (k == 2) S2 = w[i];
+              ++k;
+            }
+          if (nz) {
+            const uint32_t slot = atomicAdd(cntOut + g, 1u);
+            __stcg(entOut + (size_t)g * B + slot, make_uint4(b | (nz << 16), S0, S1, S2));
+          }
         }
-        const uint32_t wv = __ballot_sync(kFull, any);
-        if (lane == 0) __stcg(actOut + (size_t)b * nactw + (gb >> 5), wv);
       }
       if (tid == 0 && d.theta && t + 1u == c.T) d.theta[b] = theta;
       __syncthreads();
@@ -208,10 +349,14 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
   }
 }
 
-size_t recall_smem_bytes(uint32_t ncol) { return (3ull * ncol + 256 + 96 + 4) * 4; }
+size_t recall_smem_bytes(uint32_t ncol, uint32_t B, uint32_t acc32) {
+  (void)ncol;
+  const size_t stride = acc32 ? 33 : 17;
+  return (2ull * kItemWords + kRecallCpi * (size_t)B * stride + 64 + 68 + 16 + 4) * 4;
+}
 
 cudaError_t recall_max_blocks_per_sm(int acc32, int threads, size_t smem, int* out) {
-  const void* fn = acc32 ? (const void*)k_recall<uint32_t> : (const void*)k_recall<uint16_t>;
+  const void* fn = acc32 ? (const void*)k_recall<false> : (const void*)k_recall<true>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, fn, threads, smem);
@@ -219,7 +364,7 @@ cudaError_t recall_max_blocks_per_sm(int acc32, int threads, size_t smem, int* o
 
 cudaError_t launch_recall(const RecallDev& d, const RecallCfg& c, const RecallShape& s, cudaStream_t st) {
   void* args[] = {(void*)&d, (void*)&c};
-  const void* fn = c.acc32 ? (const void*)k_recall<uint32_t> : (const void*)k_recall<uint16_t>;
+  const void* fn = c.acc32 ? (const void*)k_recall<false> : (const void*)k_recall<true>;
   return cudaLaunchCooperativeKernel(fn, dim3(s.grid), dim3(s.threads), args, s.smem, st);
 }
 

@@ -6,16 +6,20 @@
 
 namespace axon {
 
+constexpr uint32_t kRecallMaxB = 512;   // trajectories per launch (the host splits larger batches)
+constexpr uint32_t kRecallCpi = 2;      // columns per phase-1 work item
+
 // Device buffers of one batched recall launch over B trajectories of one network.
 struct RecallDev {
-  const uint32_t* W3B;      // W3 re-laid out [col][branch][word][lane] (read-only during recall)
+  const uint32_t* W3R;      // W3 re-laid out [col][branch][row][word] (read-only during recall)
   const uint32_t* conn;     // [ncol*32]
   const uint32_t* bias;     // [N]
   const uint32_t* mult;     // [N]
   const uint32_t* stims;    // [B][ncol] clamp patterns
   const uint32_t* refBall;  // [B][ncol] logged reference assemblies, or null
   uint32_t* spk;            // [2][B][ncol] spike vectors by step parity (slot 0 zeroed before launch)
-  uint32_t* act;            // [2][B][nactw] group-activity bits by step parity (slot 0 zeroed)
+  uint4* ent;               // [2][ngrp][B] per-group lists of (trajectory, nonzero spike words)
+  uint32_t* ecnt;           // [2][ngrp] list lengths (slot 0 zeroed before launch)
   uint32_t* drv;            // [B][ncol] column drives of the current step
   void* acc;                // [B][ncol][32] per-neuron drive (u16 or u32) of the current step
   uint32_t* finalOut;       // [B][ncol] spikes of the last step, or null
@@ -30,8 +34,7 @@ struct RecallDev {
 
 struct RecallCfg {
   uint32_t ncol, incols, B, T, clampSteps, useBias, k, dthr, boost, mode, targetCols, facil, biasShift, topkPar;
-  uint32_t cpi;   // columns per phase-1 work item
-  uint32_t acc32; // 1: per-neuron drive kept as u32, 0: as u16
+  uint32_t acc32;  // 1: per-neuron drive kept as u32 (packing two 16-bit sums would overflow)
   uint64_t waitNs;
 };
 
@@ -40,10 +43,10 @@ struct RecallShape {
   size_t smem;
 };
 
-size_t recall_smem_bytes(uint32_t ncol);
+size_t recall_smem_bytes(uint32_t ncol, uint32_t B, uint32_t acc32);
 cudaError_t recall_max_blocks_per_sm(int acc32, int threads, size_t smem, int* out);
 cudaError_t launch_recall(const RecallDev& d, const RecallCfg& c, const RecallShape& s, cudaStream_t st);
-// W3 [col][s][j][lane][comp] -> W3B [col][s][word = 4j + comp][lane]
-cudaError_t launch_make_w3b(const uint4* W3, uint32_t* W3B, uint32_t ncol, cudaStream_t st);
+// W3 [col][s][j][lane][comp] -> W3R [col][s][row = lane][word = 4j + comp]
+cudaError_t launch_make_w3r(const uint4* W3, uint32_t* W3R, uint32_t ncol, cudaStream_t st);
 
 }  // namespace axon

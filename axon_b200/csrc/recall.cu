@@ -42,7 +42,7 @@ axon_status axon_net::ensure_w3b() {
       return set_error(AXON_ENOMEM, "W3 batch layout allocation failed");
     }
   }
-  CK(launch_make_w3b(d.W3, w3b, ncol, stream));
+  CK(launch_make_w3r(d.W3, w3b, ncol, stream));
   w3b_valid = true;
   return AXON_OK;
 }
@@ -115,59 +115,67 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     }
     CK(cudaEventRecord(ev1, stream));
   } else {
+    if (ncol > 8192) return set_error(AXON_EINVAL, "batched recall supports ncol <= 8192; use the plain method");
     axon_status st = ensure_w3b();
     if (st != AXON_OK) return st;
-    const uint32_t ngrp = ncol / 8u, nactw = (((ngrp + 31u) / 32u) + 3u) & ~3u;
+    const uint32_t ngrp = ncol / 8u;
     const PresentCfg pc = present_cfg(a.T, a.clamp_steps, false, a.use_bias);
     RecallCfg rc{};
-    rc.ncol = ncol; rc.incols = cfg.incols; rc.B = B; rc.T = a.T; rc.clampSteps = a.clamp_steps;
+    rc.ncol = ncol; rc.incols = cfg.incols; rc.T = a.T; rc.clampSteps = a.clamp_steps;
     rc.useBias = pc.useBias; rc.k = pc.k; rc.dthr = pc.dthr; rc.boost = pc.boost; rc.mode = pc.mode;
     rc.targetCols = pc.targetCols; rc.facil = pc.facil; rc.biasShift = pc.biasShift; rc.topkPar = pc.topkPar;
     rc.waitNs = wait_ns;
-    // per-neuron drive fits 16 bits unless branches can add more than 65535 in total
+    // per-neuron drive fits 16 bits (and two of them one 32-bit shared counter) unless the
+    // branches of one neuron can add up to more than 65535
     const uint64_t maxAcc = (cfg.mode == 2 ? 32ull : 32ull * (256ull + cfg.boost)) + cfg.facil;
     rc.acc32 = maxAcc > 65535ull ? 1u : 0u;
-    uint32_t cpi = 1;
-    while (cpi < 32 && (uint64_t)cpi * 2 * B <= 32) cpi *= 2;
-    rc.cpi = cpi;
-    const size_t accBytes = bn * 32 * (rc.acc32 ? 4 : 2);
-    const size_t need = al(2 * bn * 4) + al(2ull * B * nactw * 4) + al(bn * 4) + al(accBytes) + al(64 * 4);
+    const uint32_t maxB = rc.acc32 ? 300u : kRecallMaxB;
+    const uint32_t Bc = std::min(B, maxB);  // trajectories per launch
+    const size_t bnc = (size_t)Bc * ncol;
+    const size_t accBytes = bnc * 32 * (rc.acc32 ? 4 : 2);
+    const size_t need = al(2 * bnc * 4) + al(2ull * ngrp * Bc * 16) + al(2ull * ngrp * 4) + al(bnc * 4) +
+                        al(accBytes) + al(64 * 4);
     st = scratch.ensure(need);
     if (st != AXON_OK) return st;
     char* p = (char*)scratch.p;
     auto take = [&](size_t bytes) { char* r = p; p += al(bytes); return r; };
     RecallDev rd{};
-    rd.W3B = w3b;
+    rd.W3R = w3b;
     rd.conn = d.conn;
     rd.bias = d.bias;
     rd.mult = d.mult;
-    rd.stims = dCues;
-    rd.refBall = dRef;
-    rd.spk = (uint32_t*)take(2 * bn * 4);
-    rd.act = (uint32_t*)take(2ull * B * nactw * 4);
-    rd.drv = (uint32_t*)take(bn * 4);
+    rd.spk = (uint32_t*)take(2 * bnc * 4);
+    rd.ent = (uint4*)take(2ull * ngrp * Bc * 16);
+    rd.ecnt = (uint32_t*)take(2ull * ngrp * 4);
+    rd.drv = (uint32_t*)take(bnc * 4);
     rd.acc = take(accBytes);
     rd.work = (uint32_t*)take(64 * 4);
-    rd.finalOut = dFinal;
-    rd.hist = dHist;
-    rd.stats = dStats;
-    rd.driveLog = dLog;
     rd.theta = nullptr;
     rd.bar = d.bar;
     rd.err = d.err;
-    CK(cudaMemsetAsync(rd.spk, 0, bn * 4, stream));
-    CK(cudaMemsetAsync(rd.act, 0, (size_t)B * nactw * 4, stream));
-    CK(cudaMemsetAsync(rd.work, 0, 64 * 4, stream));
-    CK(cudaMemsetAsync(d.bar, 0, 4, stream));
     RecallShape rs{};
     rs.threads = 1024;
-    rs.smem = recall_smem_bytes(ncol);
+    rs.smem = recall_smem_bytes(ncol, Bc, rc.acc32);
     int per_sm = 0;
     CK(recall_max_blocks_per_sm(rc.acc32, rs.threads, rs.smem, &per_sm));
     if (per_sm < 1) return set_error(AXON_EINVAL, "batched recall kernel does not fit one SM");
     rs.grid = sm_count * per_sm;
     CK(cudaEventRecord(ev0, stream));
-    CK(launch_recall(rd, rc, rs, stream));
+    for (uint32_t b0 = 0; b0 < B; b0 += Bc) {  // one launch per chunk of trajectories
+      const uint32_t nb = std::min(Bc, B - b0);
+      rc.B = nb;
+      rd.stims = dCues + (size_t)b0 * ncol;
+      rd.refBall = dRef ? dRef + (size_t)b0 * ncol : nullptr;
+      rd.finalOut = dFinal ? dFinal + (size_t)b0 * ncol : nullptr;
+      rd.hist = dHist ? dHist + (size_t)b0 * a.T * ncol : nullptr;
+      rd.stats = dStats ? dStats + (size_t)b0 * 1024 : nullptr;
+      rd.driveLog = dLog ? dLog + (size_t)b0 * 256 : nullptr;
+      CK(cudaMemsetAsync(rd.spk, 0, (size_t)nb * ncol * 4, stream));
+      CK(cudaMemsetAsync(rd.ecnt, 0, ngrp * 4, stream));
+      CK(cudaMemsetAsync(rd.work, 0, 64 * 4, stream));
+      CK(cudaMemsetAsync(d.bar, 0, 4, stream));
+      CK(launch_recall(rd, rc, rs, stream));
+    }
     CK(cudaEventRecord(ev1, stream));
   }
   axon_status st = check_device_error();
