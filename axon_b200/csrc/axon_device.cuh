@@ -97,6 +97,16 @@ __device__ __forceinline__ uint32_t warp_kwta(uint32_t v, uint32_t lane, uint32_
   return __ballot_sync(kFull, rank < k);
 }
 
+// ---------------------------------------------------------------- asynchronous copies
+// 16-byte global->shared copies that bypass L1 (the source was written by other SMs)
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // ---------------------------------------------------------------- bounded grid barrier
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;

@@ -25,15 +25,21 @@
 
 namespace axon {
 
+// Tile layout for the batched kernel: word w of row r of a (column, branch) tile is stored
+// at w*32 + ((r + 4w) mod 32). Rows r..r+3 (r a multiple of 4) of one word are then 16
+// contiguous bytes, and lanes reading different words hit different groups of 4 banks.
+__host__ __device__ __forceinline__ uint32_t w3r_pos(uint32_t r, uint32_t w) { return w * 32u + ((r + 4u * w) & 31u); }
+
 __global__ void k_make_w3r(const uint4* __restrict__ W3, uint32_t* __restrict__ W3R, uint64_t ntile) {
-  // one thread per (tile, row): the row's two uint4 halves become 8 consecutive words
+  // one thread per (tile, row): scatters the row's 8 words
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ntile * 32) return;
   const uint64_t tile = i >> 5;
   const uint32_t row = (uint32_t)(i & 31u);
-  uint4* o = reinterpret_cast<uint4*>(W3R + tile * 256 + row * 8);
-  o[0] = W3[tile * kTileU4 + row];
-  o[1] = W3[tile * kTileU4 + 32 + row];
+  const uint4 a = W3[tile * kTileU4 + row], b = W3[tile * kTileU4 + 32 + row];
+  uint32_t* o = W3R + tile * 256;
+  o[w3r_pos(row, 0)] = a.x; o[w3r_pos(row, 1)] = a.y; o[w3r_pos(row, 2)] = a.z; o[w3r_pos(row, 3)] = a.w;
+  o[w3r_pos(row, 4)] = b.x; o[w3r_pos(row, 5)] = b.y; o[w3r_pos(row, 6)] = b.z; o[w3r_pos(row, 7)] = b.w;
 }
 
 cudaError_t launch_make_w3r(const uint4* W3, uint32_t* W3R, uint32_t ncol, cudaStream_t st) {
@@ -76,34 +82,50 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64
   }
 }
 
-// dendritic nonlinearity of k_drive, src/axon.mm:174-178 (applied to non-silent branches)
-__device__ __forceinline__ uint32_t branch_term(uint32_t cnt, const RecallCfg& c) {
-  const bool nmda = cnt >= c.dthr;
-  if (c.mode == 0u) return cnt;
-  if (c.mode == 1u) return nmda ? cnt + c.boost : cnt;
-  return nmda ? 1u : 0u;
+// dendritic nonlinearity of k_drive, src/axon.mm:174-178, applied to a non-silent branch.
+// LIN (modes 0, 1): count plus bst when the count reaches dthr; otherwise (mode 2) 0 or 1.
+template <bool LIN>
+__device__ __forceinline__ uint32_t branch_term(uint32_t cnt, uint32_t dthr, uint32_t bst) {
+  if (LIN) return cnt + (cnt >= dthr ? bst : 0u);
+  return cnt >= dthr ? 1u : 0u;
 }
 
-constexpr uint32_t kColWords = kNslot * 256;           // one column's 32 tiles, [branch][row][word]
+constexpr uint32_t kColWords = kNslot * 256;             // one column's 32 tiles
 constexpr uint32_t kItemWords = kRecallCpi * kColWords;  // one work item
 
 template <bool PACK>
+__device__ __forceinline__ void acc_add4(uint32_t* accb, uint32_t r, uint32_t t0, uint32_t t1, uint32_t t2,
+                                         uint32_t t3) {
+  if (PACK) {
+    atomicAdd(accb + (r >> 1), t0 | (t1 << 16));
+    atomicAdd(accb + (r >> 1) + 1, t2 | (t3 << 16));
+  } else {
+    atomicAdd(accb + r, t0);
+    atomicAdd(accb + r + 1, t1);
+    atomicAdd(accb + r + 2, t2);
+    atomicAdd(accb + r + 3, t3);
+  }
+}
+
+template <bool PACK, bool LIN>
 __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
   extern __shared__ __align__(128) uint32_t sm[];
   const uint32_t ncol = c.ncol, incols = c.incols, B = c.B, ngrp = ncol / 8u;
+  const uint32_t dthr = c.dthr, bst = c.bst;
   constexpr uint32_t accStride = PACK ? 17u : 33u;  // padded: distinct trajectories hit distinct banks
   uint32_t* sTile = sm;                                  // [2][kItemWords]
   uint32_t* sAcc = sTile + 2 * kItemWords;               // [kRecallCpi][B][accStride]
   uint32_t* sConn = sAcc + kRecallCpi * B * accStride;   // [64]
-  uint32_t* sP = sConn + 64;                             // [68] entry prefix over the item's 64 branches
-  uint32_t* sMisc = sP + 68;                             // [16]
+  uint32_t* sP1 = sConn + 64;                            // [68] single-word entries: prefix over 64 branches
+  uint32_t* sPM = sP1 + 68;                              // [68] multi-word entries
+  uint32_t* sMisc = sPM + 68;                            // [16]
   uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
   // phase-2 views reuse the tile buffers
   uint32_t* sD = sTile;
   uint32_t* sSpk = sTile + ncol;
   uint32_t* sList = sTile + 2 * ncol;
-  uint32_t* sHist = sTile + 3 * ncol;
-  uint32_t* sRed = sHist + 256;
+  uint32_t* sRed = sTile + 3 * ncol;  // 192 words
+  uint32_t* sHist = sRed + 192;
 
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
   const uint32_t nitems = (ncol + kRecallCpi - 1) / kRecallCpi;
@@ -120,9 +142,8 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
   auto issue = [&](uint32_t item, uint32_t buf) {  // thread 0 only
     const uint32_t c0 = item * kRecallCpi;
     const uint32_t ncols = min(kRecallCpi, ncol - c0);
-    const uint32_t bytes = ncols * kColWords * 4u;
     fence_proxy_async_smem();
-    mbar_expect_tx(&sBar[buf], bytes);
+    mbar_expect_tx(&sBar[buf], ncols * kColWords * 4u);
     for (uint32_t k = 0; k < ncols; ++k)
       bulk_g2s(sTile + buf * kItemWords + k * kColWords, d.W3R + (size_t)(c0 + k) * kColWords, kColWords * 4u, &sBar[buf]);
   };
@@ -131,15 +152,19 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
     const uint32_t par = t & 1u;
     const uint32_t* spkIn = d.spk + (size_t)par * B * ncol;
     uint32_t* spkOut = d.spk + (size_t)(par ^ 1u) * B * ncol;
-    const uint4* entIn = d.ent + (size_t)par * ngrp * B;
-    uint4* entOut = d.ent + (size_t)(par ^ 1u) * ngrp * B;
-    const uint32_t* cntIn = d.ecnt + par * ngrp;
-    uint32_t* cntOut = d.ecnt + (par ^ 1u) * ngrp;
+    const uint2* e1In = d.ent1 + (size_t)par * ngrp * B;
+    const uint4* eMIn = d.entM + (size_t)par * ngrp * B;
+    uint2* e1Out = d.ent1 + (size_t)(par ^ 1u) * ngrp * B;
+    uint4* eMOut = d.entM + (size_t)(par ^ 1u) * ngrp * B;
+    const uint32_t* c1In = d.ecnt + (size_t)par * 2 * ngrp;
+    const uint32_t* cMIn = c1In + ngrp;
+    uint32_t* c1Out = d.ecnt + (size_t)(par ^ 1u) * 2 * ngrp;
+    uint32_t* cMOut = c1Out + ngrp;
     const bool clamp = t < c.clampSteps;
 
     // next step's list lengths start at zero (last read in phase 1 of step t-1)
     if (blockIdx.x == 0)
-      for (uint32_t g = tid; g < ngrp; g += blockDim.x) cntOut[g] = 0u;
+      for (uint32_t g = tid; g < 2 * ngrp; g += blockDim.x) c1Out[g] = 0u;
 
     // ---------------- phase 1
     if (tid == 0) {
@@ -164,9 +189,11 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
       }
       for (uint32_t i = tid; i < kRecallCpi * B * accStride; i += blockDim.x) sAcc[i] = 0u;
       __syncthreads();
-      if (warp == 0) {  // prefix of the 64 list lengths
-        const bool v0 = c0 < ncol, v1 = c0 + 1 < ncol;
-        const uint32_t n0 = v0 ? __ldcg(cntIn + sConn[lane]) : 0u, n1 = v1 ? __ldcg(cntIn + sConn[32 + lane]) : 0u;
+      if (warp < 2) {  // prefixes of the 64 list lengths, single-word (warp 0) and multi-word (warp 1)
+        const uint32_t* cin = warp ? cMIn : c1In;
+        uint32_t* P = warp ? sPM : sP1;
+        const bool v1 = c0 + 1 < ncol;
+        const uint32_t n0 = __ldcg(cin + sConn[lane]), n1 = v1 ? __ldcg(cin + sConn[32 + lane]) : 0u;
         uint32_t i0 = n0, i1 = n1;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
@@ -174,9 +201,9 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
           if (lane >= (uint32_t)off) { i0 += a; i1 += b; }
         }
         const uint32_t tot0 = __shfl_sync(kFull, i0, 31);
-        sP[1 + lane] = i0;
-        sP[33 + lane] = tot0 + i1;
-        if (lane == 0) sP[0] = 0u;
+        P[1 + lane] = i0;
+        P[33 + lane] = tot0 + i1;
+        if (lane == 0) P[0] = 0u;
       }
       const bool ok = mbar_wait(&sBar[bcur], (bcur ? uses1 : uses0) & 1u, c.waitNs);
       if (bcur) ++uses1; else ++uses0;
@@ -185,41 +212,40 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
         mbar_wait(&sBar[bcur ^ 1u], (bcur ? uses0 : uses1) & 1u, c.waitNs);  // copies still in flight
         return;
       }
-      const uint32_t E = sP[64], units = (E + 31u) >> 5;
+      const uint32_t E1 = sP1[64], E = E1 + sPM[64], units = (E + 31u) >> 5;
       const uint32_t* tileBase = sTile + bcur * kItemWords;
       for (;;) {
         uint32_t u = 0;
         if (lane == 0) u = atomicAdd(sMisc + 3, 1u);
         u = __shfl_sync(kFull, u, 0);
         if (u >= units) break;
-        const uint32_t flat = u * 32u + lane;
+        uint32_t flat = u * 32u + lane;
         if (flat >= E) continue;
+        const bool single = flat < E1;
+        const uint32_t* P = single ? sP1 : sPM;
+        if (!single) flat -= E1;
         uint32_t sp = 0;
 #pragma unroll
         for (uint32_t step = 32; step; step >>= 1)
-          if (sp + step < 64u && sP[sp + step] <= flat) sp += step;
-        const uint32_t e = flat - sP[sp];
+          if (sp + step < 64u && P[sp + step] <= flat) sp += step;
+        const uint32_t e = flat - P[sp];
         const uint32_t g = sConn[sp];
-        const uint4 en = __ldcg(entIn + (size_t)g * B + e);
-        const uint32_t b = en.x & 0xFFFFu, nz = (en.x >> 16) & 0xFFu;
         const uint32_t* tile = tileBase + (sp >> 5) * kColWords + (sp & 31u) * 256u;
-        uint32_t* accb = sAcc + ((sp >> 5) * B + b) * accStride;
-        const uint32_t w0 = (uint32_t)__ffs(nz) - 1u;
-        const uint32_t nz1 = nz & (nz - 1u);
-        const uint32_t nz2 = nz1 & (nz1 - 1u);
-        if (nz2 == 0u) {  // one or two nonzero words: the common case
-          const uint32_t w1 = nz1 ? (uint32_t)__ffs(nz1) - 1u : w0;
-          const uint32_t S0 = en.y, S1 = nz1 ? en.z : 0u;
+        if (single) {  // one nonzero word: 32 AND-counts
+          const uint2 en = __ldcg(e1In + (size_t)g * B + e);
+          const uint32_t b = en.x & 0xFFFFu, w = en.x >> 16, S = en.y;
+          uint32_t* accb = sAcc + ((sp >> 5) * B + b) * accStride;
 #pragma unroll 4
-          for (uint32_t r = 0; r < 32u; r += 2) {
-            const uint32_t* ra = tile + r * 8u;
-            const uint32_t q0 = __popc(ra[w0] & S0) + __popc(ra[w1] & S1);
-            const uint32_t q1 = __popc(ra[8 + w0] & S0) + __popc(ra[8 + w1] & S1);
-            const uint32_t t0 = branch_term(q0, c), t1 = branch_term(q1, c);
-            if (PACK) atomicAdd(accb + (r >> 1), t0 | (t1 << 16));
-            else { atomicAdd(accb + r, t0); atomicAdd(accb + r + 1, t1); }
+          for (uint32_t r = 0; r < 32u; r += 4) {
+            const uint4 a = *reinterpret_cast<const uint4*>(tile + w3r_pos(r, w));
+            acc_add4<PACK>(accb, r, branch_term<LIN>(__popc(a.x & S), dthr, bst),
+                           branch_term<LIN>(__popc(a.y & S), dthr, bst), branch_term<LIN>(__popc(a.z & S), dthr, bst),
+                           branch_term<LIN>(__popc(a.w & S), dthr, bst));
           }
-        } else {  // three or more nonzero words: counts in registers, words past the third from the spikes
+        } else {  // several nonzero words: counts in registers (words past the third from the spikes)
+          const uint4 en = __ldcg(eMIn + (size_t)g * B + e);
+          const uint32_t b = en.x & 0xFFFFu, nz = (en.x >> 16) & 0xFFu;
+          uint32_t* accb = sAcc + ((sp >> 5) * B + b) * accStride;
           uint32_t cnt[32];
 #pragma unroll
           for (int r = 0; r < 32; ++r) cnt[r] = 0u;
@@ -230,41 +256,56 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
             const uint32_t S = k == 0 ? en.y : k == 1 ? en.z : k == 2 ? en.w : __ldcg(spkIn + (size_t)b * ncol + 8u * g + w);
             ++k;
 #pragma unroll
-            for (int r = 0; r < 32; ++r) cnt[r] += __popc(tile[r * 8 + w] & S);
+            for (int r = 0; r < 32; r += 4) {
+              const uint4 a = *reinterpret_cast<const uint4*>(tile + w3r_pos(r, w));
+              cnt[r] += __popc(a.x & S); cnt[r + 1] += __popc(a.y & S);
+              cnt[r + 2] += __popc(a.z & S); cnt[r + 3] += __popc(a.w & S);
+            }
           }
 #pragma unroll
-          for (int r = 0; r < 32; r += 2) {
-            const uint32_t t0 = branch_term(cnt[r], c), t1 = branch_term(cnt[r + 1], c);
-            if (PACK) atomicAdd(accb + (r >> 1), t0 | (t1 << 16));
-            else { atomicAdd(accb + r, t0); atomicAdd(accb + r + 1, t1); }
-          }
+          for (int r = 0; r < 32; r += 4)
+            acc_add4<PACK>(accb, r, branch_term<LIN>(cnt[r], dthr, bst), branch_term<LIN>(cnt[r + 1], dthr, bst),
+                           branch_term<LIN>(cnt[r + 2], dthr, bst), branch_term<LIN>(cnt[r + 3], dthr, bst));
         }
       }
       __syncthreads();
       // per-neuron and column drives of the item's columns for every trajectory
-      for (uint32_t pp = warp; pp < kRecallCpi * B; pp += nw) {
-        const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
-        if (col >= ncol) continue;
-        const uint32_t* ab = sAcc + (colL * B + b) * accStride;
-        uint32_t a = PACK ? ((ab[lane >> 1] >> (16u * (lane & 1u))) & 0xFFFFu) : ab[lane];
-        if (c.facil != 0u && ((__ldcg(spkIn + (size_t)b * ncol + col) >> lane) & 1u)) a += c.facil;
-        const uint32_t biasL = c.useBias ? (__ldg(d.bias + col * 32u + lane) >> c.biasShift) : 0u;
-        a = a > biasL ? a - biasL : 0u;
-        if (c.acc32) reinterpret_cast<uint32_t*>(d.acc)[((size_t)b * ncol + col) * 32u + lane] = a;
-        else reinterpret_cast<uint16_t*>(d.acc)[((size_t)b * ncol + col) * 32u + lane] = (uint16_t)a;
-        const uint32_t dsum = __reduce_add_sync(kFull, a);
-        if (lane == 0) __stcg(d.drv + (size_t)b * ncol + col, dsum);
-        if (d.refBall != nullptr && col >= incols) {  // driveLog of k_emit, src/axon.mm:216-220
-          const uint32_t rb = __ldg(d.refBall + (size_t)b * ncol + col);
-          if (rb) {
-            const bool member = (rb >> lane) & 1u, shared = __ldg(d.mult + col * 32u + lane) > 1u;
-            const uint32_t mS = __ballot_sync(kFull, member && shared), mE = __ballot_sync(kFull, member && !shared);
-            const uint32_t sumS = __reduce_add_sync(kFull, (member && shared) ? a : 0u);
-            const uint32_t sumE = __reduce_add_sync(kFull, (member && !shared) ? a : 0u);
-            if (lane == 0) {
-              uint32_t* dl = d.driveLog + (size_t)b * 256u + t * 4u;
-              if (mS) { atomicAdd(dl + 0, sumS); atomicAdd(dl + 1, (uint32_t)__popc(mS)); }
-              if (mE) { atomicAdd(dl + 2, sumE); atomicAdd(dl + 3, (uint32_t)__popc(mE)); }
+      if (PACK && !c.useBias && !c.facil && d.refBall == nullptr) {
+        // the packed counters already are the u16 drive slab: half a warp per (column, trajectory)
+        const uint32_t half = lane >> 4, l16 = lane & 15u;
+        for (uint32_t pp = warp * 2u + half; pp < kRecallCpi * B; pp += nw * 2u) {
+          const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
+          if (col >= ncol) continue;  // uniform over the half warp
+          const uint32_t w = sAcc[(colL * B + b) * accStride + l16];
+          reinterpret_cast<uint32_t*>(d.acc)[(((size_t)b * ncol + col) * 32u >> 1) + l16] = w;
+          const uint32_t dsum = __reduce_add_sync(half ? 0xFFFF0000u : 0x0000FFFFu, (w & 0xFFFFu) + (w >> 16));
+          if (l16 == 0) __stcg(d.drv + (size_t)b * ncol + col, dsum);
+        }
+      } else {
+        for (uint32_t pp = warp; pp < kRecallCpi * B; pp += nw) {
+          const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
+          if (col >= ncol) continue;
+          const uint32_t* ab = sAcc + (colL * B + b) * accStride;
+          uint32_t a = PACK ? ((ab[lane >> 1] >> (16u * (lane & 1u))) & 0xFFFFu) : ab[lane];
+          if (c.facil != 0u && ((__ldcg(spkIn + (size_t)b * ncol + col) >> lane) & 1u)) a += c.facil;
+          const uint32_t biasL = c.useBias ? (__ldg(d.bias + col * 32u + lane) >> c.biasShift) : 0u;
+          a = a > biasL ? a - biasL : 0u;
+          if (c.acc32) reinterpret_cast<uint32_t*>(d.acc)[((size_t)b * ncol + col) * 32u + lane] = a;
+          else reinterpret_cast<uint16_t*>(d.acc)[((size_t)b * ncol + col) * 32u + lane] = (uint16_t)a;
+          const uint32_t dsum = __reduce_add_sync(kFull, a);
+          if (lane == 0) __stcg(d.drv + (size_t)b * ncol + col, dsum);
+          if (d.refBall != nullptr && col >= incols) {  // driveLog of k_emit, src/axon.mm:216-220
+            const uint32_t rb = __ldg(d.refBall + (size_t)b * ncol + col);
+            if (rb) {
+              const bool member = (rb >> lane) & 1u, shared = __ldg(d.mult + col * 32u + lane) > 1u;
+              const uint32_t mS = __ballot_sync(kFull, member && shared), mE = __ballot_sync(kFull, member && !shared);
+              const uint32_t sumS = __reduce_add_sync(kFull, (member && shared) ? a : 0u);
+              const uint32_t sumE = __reduce_add_sync(kFull, (member && !shared) ? a : 0u);
+              if (lane == 0) {
+                uint32_t* dl = d.driveLog + (size_t)b * 256u + t * 4u;
+                if (mS) { atomicAdd(dl + 0, sumS); atomicAdd(dl + 1, (uint32_t)__popc(mS)); }
+                if (mE) { atomicAdd(dl + 2, sumE); atomicAdd(dl + 3, (uint32_t)__popc(mE)); }
+              }
             }
           }
         }
@@ -282,7 +323,7 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
         reinterpret_cast<uint4*>(sD)[i] = __ldcg(reinterpret_cast<const uint4*>(drvb) + i);
       if (tid == 0) sMisc[4] = 0u;
       __syncthreads();
-      const uint32_t theta = block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed);
+      const uint32_t theta = block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed, __ldcg(d.thPrev + b));
       const uint32_t gate = max(theta, 1u);
       const uint32_t* stimb = d.stims + (size_t)b * ncol;
       for (uint32_t cc = tid; cc < ncol; cc += blockDim.x) {
@@ -326,23 +367,29 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
         for (uint32_t g = tid; g < ngrp; g += blockDim.x) {
           const uint4 p = reinterpret_cast<const uint4*>(sSpk)[2 * g], q = reinterpret_cast<const uint4*>(sSpk)[2 * g + 1];
           const uint32_t w[8] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w};
-          uint32_t nz = 0, S0 = 0u, S1 = 0u, S2 = 0u, k = 0;
+          uint32_t nz = 0, S0 = 0u, S1 = 0u, S2 = 0u, k = 0, w0 = 0;
 #pragma unroll
           for (int i = 0; i < 8; ++i)
             if (w[i]) {
               nz |= 1u << i;
-              if (k == 0) S0 = w[i];
+              if (k == 0) { S0 = w[i]; w0 = (uint32_t)i; }
               else if (k == 1) S1 = w[i];
               else if (k == 2) S2 = w[i];
               ++k;
             }
-          if (nz) {
-            const uint32_t slot = atomicAdd(cntOut + g, 1u);
-            __stcg(entOut + (size_t)g * B + slot, make_uint4(b | (nz << 16), S0, S1, S2));
+          if (k == 1) {
+            const uint32_t slot = atomicAdd(c1Out + g, 1u);
+            __stcg(e1Out + (size_t)g * B + slot, make_uint2(b | (w0 << 16), S0));
+          } else if (k > 1) {
+            const uint32_t slot = atomicAdd(cMOut + g, 1u);
+            __stcg(eMOut + (size_t)g * B + slot, make_uint4(b | (nz << 16), S0, S1, S2));
           }
         }
       }
-      if (tid == 0 && d.theta && t + 1u == c.T) d.theta[b] = theta;
+      if (tid == 0) {
+        __stcg(d.thPrev + b, theta);
+        if (d.theta && t + 1u == c.T) d.theta[b] = theta;
+      }
       __syncthreads();
     }
     if (t + 1u < c.T && !grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;
@@ -352,20 +399,28 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
 size_t recall_smem_bytes(uint32_t ncol, uint32_t B, uint32_t acc32) {
   (void)ncol;
   const size_t stride = acc32 ? 33 : 17;
-  return (2ull * kItemWords + kRecallCpi * (size_t)B * stride + 64 + 68 + 16 + 4) * 4;
+  return (2ull * kItemWords + kRecallCpi * (size_t)B * stride + 64 + 68 + 68 + 16 + 4) * 4;
 }
 
+namespace {
+const void* recall_fn(uint32_t acc32, uint32_t lin) {
+  if (acc32) return lin ? (const void*)k_recall<false, true> : (const void*)k_recall<false, false>;
+  return lin ? (const void*)k_recall<true, true> : (const void*)k_recall<true, false>;
+}
+}  // namespace
+
 cudaError_t recall_max_blocks_per_sm(int acc32, int threads, size_t smem, int* out) {
-  const void* fn = acc32 ? (const void*)k_recall<false> : (const void*)k_recall<true>;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, fn, threads, smem);
+  for (uint32_t lin = 0; lin < 2; ++lin) {
+    cudaError_t e = cudaFuncSetAttribute(recall_fn(acc32, lin), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, recall_fn(acc32, 1), threads, smem);
 }
 
 cudaError_t launch_recall(const RecallDev& d, const RecallCfg& c, const RecallShape& s, cudaStream_t st) {
   void* args[] = {(void*)&d, (void*)&c};
-  const void* fn = c.acc32 ? (const void*)k_recall<false> : (const void*)k_recall<true>;
-  return cudaLaunchCooperativeKernel(fn, dim3(s.grid), dim3(s.threads), args, s.smem, st);
+  return cudaLaunchCooperativeKernel(recall_fn(c.acc32, c.mode != 2u), dim3(s.grid), dim3(s.threads), args, s.smem,
+                                     st);
 }
 
 }  // namespace axon

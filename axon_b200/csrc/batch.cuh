@@ -18,8 +18,9 @@ struct RecallDev {
   const uint32_t* stims;    // [B][ncol] clamp patterns
   const uint32_t* refBall;  // [B][ncol] logged reference assemblies, or null
   uint32_t* spk;            // [2][B][ncol] spike vectors by step parity (slot 0 zeroed before launch)
-  uint4* ent;               // [2][ngrp][B] per-group lists of (trajectory, nonzero spike words)
-  uint32_t* ecnt;           // [2][ngrp] list lengths (slot 0 zeroed before launch)
+  uint2* ent1;              // [2][ngrp][B] per-group lists of trajectories with ONE nonzero spike word
+  uint4* entM;              // [2][ngrp][B] per-group lists of trajectories with several nonzero words
+  uint32_t* ecnt;           // [2 parity][2 lists][ngrp] list lengths (parity 0 zeroed before launch)
   uint32_t* drv;            // [B][ncol] column drives of the current step
   void* acc;                // [B][ncol][32] per-neuron drive (u16 or u32) of the current step
   uint32_t* finalOut;       // [B][ncol] spikes of the last step, or null
@@ -27,6 +28,7 @@ struct RecallDev {
   uint32_t* stats;          // [B][1024] counters (zeroed before launch), or null
   uint32_t* driveLog;       // [B][256] member-drive log (accumulated), or null
   uint32_t* theta;          // [B] threshold of the last step, or null
+  uint32_t* thPrev;         // [B] each trajectory's latest threshold (zeroed before launch)
   uint32_t* work;           // [T] phase-1 work counters (zeroed before launch)
   uint32_t* bar;            // grid barrier counter (zeroed before launch)
   uint32_t* err;            // device error word
@@ -35,6 +37,7 @@ struct RecallDev {
 struct RecallCfg {
   uint32_t ncol, incols, B, T, clampSteps, useBias, k, dthr, boost, mode, targetCols, facil, biasShift, topkPar;
   uint32_t acc32;  // 1: per-neuron drive kept as u32 (packing two 16-bit sums would overflow)
+  uint32_t bst;    // dendritic bonus per branch at or above dthr: boost (mode 1), 0 (mode 0)
   uint64_t waitNs;
 };
 

@@ -88,13 +88,13 @@ axon_status axon_net::create(const axon_cfg& c, int dev) {
   cudaDeviceProp prop;
   CK(cudaGetDeviceProperties(&prop, device));
   sm_count = prop.multiProcessorCount;
-  shape.smem = present_smem_bytes(ncol, c.incols);
   bool ok = false;
   for (int cpw : {1, 2, 4}) {
     const uint32_t warps = (ncol + cpw - 1) / cpw;
     int wpb = (int)std::min<uint32_t>(32, (warps + prop.multiProcessorCount - 1) / prop.multiProcessorCount);
     wpb = std::max(wpb, 1);
     const int grid = (int)((warps + wpb - 1) / wpb);
+    shape.smem = present_smem_bytes(ncol, c.incols, cpw);
     int per_sm = 0;
     CK(present_max_blocks_per_sm(cpw, wpb * 32, shape.smem, &per_sm));
     if (per_sm >= 1 && grid <= per_sm * prop.multiProcessorCount) {

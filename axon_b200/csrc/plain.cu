@@ -58,15 +58,25 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
   uint32_t* sD = sAct1 + nactw;            // staged drives of the current step
   uint32_t* sB = sD + ncol;                // staged ungated ballots
   uint32_t* sStim = sB + ncol;             // input clamp pattern
-  uint32_t* sHist = sStim + ((incols + 3u) & ~3u);
-  uint32_t* sRed = sHist + 256;            // 96 words of reduction scratch
-  uint32_t* sFlag = sRed + 96;
-
+  uint32_t* sHist = sStim + ((incols + 3u) & ~3u);  // 256 bins of the threshold select
+  uint32_t* sRed = sHist + 256;            // 192 words of reduction scratch
+  uint32_t* sFlag = sRed + 192;            // [0] barrier flag, [1] learning-task count
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, wpb = blockDim.x >> 5;
+  const uint32_t maxCols = wpb * CPW;      // columns owned by this CTA
+  uint32_t* sTask = sFlag + 4;             // learning tasks: (column slot << 5) | branch
+  uint32_t* sBBL = sTask + maxCols * 32;   // branch-NMDA masks of the learning columns
+  uint32_t* sLTP = sBBL + maxCols * 32;    // per-neuron potentiation counts of this step
+  uint32_t* sLTD = sLTP + maxCols * 32;    // per-neuron depression counts
+  uint32_t* sFiredL = sLTD + maxCols * 32; // spike ballot of each learning column
+  uint32_t* sColL = sFiredL + maxCols;     // its column index
+  uint32_t* sMark = sColL + maxCols;       // step+1 when the slot learns this step
+
   const uint32_t gwarp = blockIdx.x * wpb + warp, nwarps = gridDim.x * wpb;
 
   for (uint32_t i = tid; i < ncol; i += blockDim.x) sSpk0[i] = 0u;
   for (uint32_t i = tid; i < nactw; i += blockDim.x) sAct0[i] = 0u;
+  for (uint32_t i = tid; i < maxCols; i += blockDim.x) sMark[i] = 0u;
+  if (tid == 0) sFlag[1] = 0u;
   for (uint32_t i = tid; i < incols; i += blockDim.x) sStim[i] = d.stim[i];
 
   // per-column state of the columns this warp owns (lane = neuron, or lane = branch for conn)
@@ -83,6 +93,7 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
     }
   }
   __syncthreads();
+  uint32_t thPrev = 0;  // last step's threshold: a starting guess for the next selection
 
   for (uint32_t t = 0; t < c.T; ++t) {
     const uint32_t* sIn = (t & 1u) ? sSpk1 : sSpk0;
@@ -96,6 +107,8 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
                            : (clamp ? 1u : (((t - c.clampSteps) % c.ltdEvery == 0u) ? 2u : 3u));
 
     // ---------------- phase A: drive (k_drive, src/axon.mm:150-190) + ungated k-WTA
+    // The owner warp walks its column's non-silent branches four at a time, so four W3
+    // tiles (2 x 512 B each) are in flight per warp; spikes come from shared memory.
 #pragma unroll
     for (int i = 0; i < CPW; ++i) {
       if (col[i] >= ncol) continue;  // warp-uniform
@@ -126,9 +139,7 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
             const uint32_t cnt = popc4(w0[u], sIn4[2 * g]) + popc4(w1[u], sIn4[2 * g + 1]);
             const bool nmda = cnt >= c.dthr;
             if (nmda) b2 |= 1u << s[u];
-            if (c.mode == 0u) a += cnt;
-            else if (c.mode == 1u) a += nmda ? cnt + c.boost : cnt;
-            else a += nmda ? 1u : 0u;
+            a += c.mode == 0u ? cnt : (c.mode == 1u ? (nmda ? cnt + c.boost : cnt) : (nmda ? 1u : 0u));
           }
       }
       if (c.facil != 0u && ((sIn[cc] >> lane) & 1u)) a += c.facil;
@@ -147,30 +158,48 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
     if (!grid_barrier(d.bar, d.err, gridDim.x, t, c.waitNs, sFlag)) return;
 
     // ---------------- phase B: column threshold (k_topk) and the full spike vector
-    for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x) {
-      reinterpret_cast<uint4*>(sD)[i] = __ldcg(reinterpret_cast<const uint4*>(d.xdrive + par * ncol) + i);
-      reinterpret_cast<uint4*>(sB)[i] = __ldcg(reinterpret_cast<const uint4*>(d.xball + par * ncol) + i);
-    }
+    // drives and ballots come from L2 by asynchronous copies; the ballots keep arriving
+    // while the threshold is selected from the drives
+    for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x)
+      cp_async16(reinterpret_cast<uint4*>(sD) + i, reinterpret_cast<const uint4*>(d.xdrive + par * ncol) + i);
+    cp_async_commit();
+    for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x)
+      cp_async16(reinterpret_cast<uint4*>(sB) + i, reinterpret_cast<const uint4*>(d.xball + par * ncol) + i);
+    cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
-    const uint32_t theta = block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed);
+    const uint32_t theta = block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed, thPrev);
+    thPrev = theta;
     const uint32_t gate = max(theta, 1u);
-    // k_emit gate and clamp, src/axon.mm:211-212
-    for (uint32_t cc = tid; cc < ncol; cc += blockDim.x) {
-      uint32_t b = sD[cc] < gate ? 0u : sB[cc];
-      if (clamp && cc < incols) b = sStim[cc];
-      sOut[cc] = b;
-    }
+    cp_async_wait<0>();
     __syncthreads();
+    // k_emit gate and clamp (src/axon.mm:211-212), one presynaptic group of 8 columns per
+    // lane, with the group-activity bit of the next step's drive
     for (uint32_t gb = warp * 32u; gb < ngrp; gb += wpb * 32u) {
       const uint32_t g = gb + lane;
       bool any = false;
       if (g < ngrp) {
-        const uint4 p = reinterpret_cast<const uint4*>(sOut)[2 * g], q = reinterpret_cast<const uint4*>(sOut)[2 * g + 1];
-        any = (p.x | p.y | p.z | p.w | q.x | q.y | q.z | q.w) != 0u;
+        const uint4* d4 = reinterpret_cast<const uint4*>(sD) + 2 * g;
+        const uint4* b4 = reinterpret_cast<const uint4*>(sB) + 2 * g;
+        uint32_t w[8];
+        const uint4 d0 = d4[0], d1 = d4[1], b0 = b4[0], b1 = b4[1];
+        w[0] = d0.x < gate ? 0u : b0.x; w[1] = d0.y < gate ? 0u : b0.y;
+        w[2] = d0.z < gate ? 0u : b0.z; w[3] = d0.w < gate ? 0u : b0.w;
+        w[4] = d1.x < gate ? 0u : b1.x; w[5] = d1.y < gate ? 0u : b1.y;
+        w[6] = d1.z < gate ? 0u : b1.z; w[7] = d1.w < gate ? 0u : b1.w;
+        if (clamp && 8u * g < incols) {
+#pragma unroll
+          for (uint32_t k = 0; k < 8u; ++k)
+            if (8u * g + k < incols) w[k] = sStim[8u * g + k];
+        }
+        reinterpret_cast<uint4*>(sOut)[2 * g] = make_uint4(w[0], w[1], w[2], w[3]);
+        reinterpret_cast<uint4*>(sOut)[2 * g + 1] = make_uint4(w[4], w[5], w[6], w[7]);
+        any = (w[0] | w[1] | w[2] | w[3] | w[4] | w[5] | w[6] | w[7]) != 0u;
       }
       const uint32_t wv = __ballot_sync(kFull, any);
       if (lane == 0) sActOut[gb >> 5] = wv;
     }
+    __syncthreads();
     if (blockIdx.x == 0 && tid == 0) { d.theta[0] = theta; d.theta[1] = 0u; }
 
     // ---------------- phase C: own-column records, bias and learning
@@ -215,17 +244,26 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
         const int nb = (int)bias[i] + (fired ? (int)c.biasUp : -dec);
         bias[i] = (uint32_t)max(0, nb);
       }
-      // k_learn, src/axon.mm:436-495
+      // k_learn, src/axon.mm:436-495: each voted branch of a learning column becomes a
+      // task that any warp of the CTA runs, so a column's read-modify-writes overlap
       if (phase == 3u || b == 0u) continue;
       if (c.marginGate != 0u && !(vk[i] > vk1[i])) continue;
+      const uint32_t slot = warp * CPW + (uint32_t)i;
       const uint32_t vmask = __reduce_or_sync(kFull, fired ? bb[i] : 0u);
-      uint32_t nLTP = 0, nLTD = 0;
-      uint32_t rem = vmask;
-      while (rem) {
-        const uint32_t s = (uint32_t)(__ffs(rem) - 1);
-        rem &= rem - 1u;
-        const bool want = fired && ((bb[i] >> s) & 1u);
-        const uint32_t g = __shfl_sync(kFull, cn[i], s);
+      sBBL[slot * 32u + lane] = bb[i];
+      sLTP[slot * 32u + lane] = 0u;
+      sLTD[slot * 32u + lane] = 0u;
+      if (lane == 0) { sFiredL[slot] = b; sColL[slot] = cc; sMark[slot] = t + 1u; }
+      if ((vmask >> lane) & 1u) sTask[atomicAdd(sFlag + 1, 1u)] = (slot << 5) | lane;
+    }
+    if (c.learn) {
+      __syncthreads();
+      const uint32_t ntask = sFlag[1];
+      for (uint32_t k = warp; k < ntask; k += wpb) {
+        const uint32_t tk = sTask[k], slot = tk >> 5, s = tk & 31u;
+        const uint32_t cc = sColL[slot];
+        const bool want = ((sFiredL[slot] >> lane) & 1u) && ((sBBL[slot * 32u + lane] >> s) & 1u);
+        const uint32_t g = __ldg(d.conn + cc * kNslot + s);
         const size_t base = ((size_t)cc * kNslot + s) * kTileU4 + lane;
         uint4 p0[2], p1[2], p2[2], p3[2];
 #pragma unroll
@@ -235,6 +273,7 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
           p2[j] = __ldcg(d.W2 + base + 32 * j);
           p3[j] = __ldcg(d.W3 + base + 32 * j);
         }
+        uint32_t nLTP = 0, nLTD = 0;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
           const uint4 sp4 = sIn4[2 * g + j];
@@ -250,15 +289,26 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
           __stcg(d.W2 + base + 32 * j, p2[j]);
           __stcg(d.W3 + base + 32 * j, p3[j]);
         }
+        if (nLTP) atomicAdd(sLTP + slot * 32u + lane, nLTP);
+        if (nLTD) atomicAdd(sLTD + slot * 32u + lane, nLTD);
       }
-      const uint32_t sLTP = __reduce_add_sync(kFull, nLTP), sLTD = __reduce_add_sync(kFull, nLTD);
-      const uint32_t kLTP = __popc(__ballot_sync(kFull, nLTP != 0u)), kLTD = __popc(__ballot_sync(kFull, nLTD != 0u));
-      if (lane == 0) {
-        if (sLTP) atomicAdd(d.stats + 8, sLTP);
-        if (sLTD) atomicAdd(d.stats + 9, sLTD);
-        if (kLTP) atomicAdd(d.stats + 10, kLTP);
-        if (kLTD) atomicAdd(d.stats + 11, kLTD);
+      __syncthreads();
+      // plasticity counters per neuron and step, src/axon.mm:491-494
+#pragma unroll
+      for (int i = 0; i < CPW; ++i) {
+        const uint32_t slot = warp * CPW + (uint32_t)i;
+        if (col[i] >= ncol || sMark[slot] != t + 1u) continue;
+        const uint32_t nLTP = sLTP[slot * 32u + lane], nLTD = sLTD[slot * 32u + lane];
+        const uint32_t sumP = __reduce_add_sync(kFull, nLTP), sumD = __reduce_add_sync(kFull, nLTD);
+        const uint32_t kP = __popc(__ballot_sync(kFull, nLTP != 0u)), kD = __popc(__ballot_sync(kFull, nLTD != 0u));
+        if (lane == 0) {
+          if (sumP) atomicAdd(d.stats + 8, sumP);
+          if (sumD) atomicAdd(d.stats + 9, sumD);
+          if (kP) atomicAdd(d.stats + 10, kP);
+          if (kD) atomicAdd(d.stats + 11, kD);
+        }
       }
+      if (tid == 0) sFlag[1] = 0u;
     }
     __syncthreads();  // sOut / sActOut complete before the next step reads them
   }
@@ -287,9 +337,11 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
 }
 
 // ---------------------------------------------------------------- launch helpers
-size_t present_smem_bytes(uint32_t ncol, uint32_t incols) {
+size_t present_smem_bytes(uint32_t ncol, uint32_t incols, int cpw) {
   const uint32_t ngrp = ncol / 8u, nactw = (((ngrp + 31u) / 32u) + 3u) & ~3u;
-  const size_t words = 2ull * ncol + 2ull * nactw + 2ull * ncol + ((incols + 3u) & ~3u) + 256 + 96 + 4;
+  const size_t maxCols = 32ull * cpw;  // upper bound of wpb * cpw
+  const size_t words = 2ull * ncol + 2ull * nactw + 2ull * ncol + ((incols + 3u) & ~3u) + 256 + 192 + 4 +
+                       maxCols * (4 * 32 + 3);
   return words * 4;
 }
 

@@ -31,7 +31,7 @@ struct LaunchShape {
   size_t smem;   // dynamic shared memory bytes
 };
 
-size_t present_smem_bytes(uint32_t ncol, uint32_t incols);
+size_t present_smem_bytes(uint32_t ncol, uint32_t incols, int cpw);
 cudaError_t present_max_blocks_per_sm(int cpw, int threads, size_t smem, int* out);
 cudaError_t launch_present(const NetDev& d, const PresentCfg& c, const LaunchShape& ls, cudaStream_t st);
 cudaError_t launch_init(const NetDev& d, uint32_t ncol, uint32_t incols, uint32_t inbr, uint32_t nand, uint32_t seed,

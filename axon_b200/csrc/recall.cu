@@ -129,12 +129,13 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     // branches of one neuron can add up to more than 65535
     const uint64_t maxAcc = (cfg.mode == 2 ? 32ull : 32ull * (256ull + cfg.boost)) + cfg.facil;
     rc.acc32 = maxAcc > 65535ull ? 1u : 0u;
+    rc.bst = cfg.mode == 1 ? cfg.boost : 0u;
     const uint32_t maxB = rc.acc32 ? 300u : kRecallMaxB;
     const uint32_t Bc = std::min(B, maxB);  // trajectories per launch
     const size_t bnc = (size_t)Bc * ncol;
     const size_t accBytes = bnc * 32 * (rc.acc32 ? 4 : 2);
-    const size_t need = al(2 * bnc * 4) + al(2ull * ngrp * Bc * 16) + al(2ull * ngrp * 4) + al(bnc * 4) +
-                        al(accBytes) + al(64 * 4);
+    const size_t need = al(2 * bnc * 4) + al(2ull * ngrp * Bc * 8) + al(2ull * ngrp * Bc * 16) + al(4ull * ngrp * 4) + al(bnc * 4) +
+                        al(accBytes) + al(64 * 4) + al((size_t)Bc * 4);
     st = scratch.ensure(need);
     if (st != AXON_OK) return st;
     char* p = (char*)scratch.p;
@@ -145,11 +146,13 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     rd.bias = d.bias;
     rd.mult = d.mult;
     rd.spk = (uint32_t*)take(2 * bnc * 4);
-    rd.ent = (uint4*)take(2ull * ngrp * Bc * 16);
-    rd.ecnt = (uint32_t*)take(2ull * ngrp * 4);
+    rd.ent1 = (uint2*)take(2ull * ngrp * Bc * 8);
+    rd.entM = (uint4*)take(2ull * ngrp * Bc * 16);
+    rd.ecnt = (uint32_t*)take(4ull * ngrp * 4);
     rd.drv = (uint32_t*)take(bnc * 4);
     rd.acc = take(accBytes);
     rd.work = (uint32_t*)take(64 * 4);
+    rd.thPrev = (uint32_t*)take((size_t)Bc * 4);
     rd.theta = nullptr;
     rd.bar = d.bar;
     rd.err = d.err;
@@ -171,8 +174,9 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
       rd.stats = dStats ? dStats + (size_t)b0 * 1024 : nullptr;
       rd.driveLog = dLog ? dLog + (size_t)b0 * 256 : nullptr;
       CK(cudaMemsetAsync(rd.spk, 0, (size_t)nb * ncol * 4, stream));
-      CK(cudaMemsetAsync(rd.ecnt, 0, ngrp * 4, stream));
+      CK(cudaMemsetAsync(rd.ecnt, 0, 2ull * ngrp * 4, stream));
       CK(cudaMemsetAsync(rd.work, 0, 64 * 4, stream));
+      CK(cudaMemsetAsync(rd.thPrev, 0, (size_t)nb * 4, stream));
       CK(cudaMemsetAsync(d.bar, 0, 4, stream));
       CK(launch_recall(rd, rc, rs, stream));
     }

@@ -109,13 +109,13 @@ extern "C" axon_status axon_present_static(const axon_cfg* cfg, const axon_state
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   LaunchShape ls{};
-  ls.smem = present_smem_bytes(ncol, cfg->incols);
   bool ok = false;
   for (int cpw : {1, 2, 4}) {
     const uint32_t warps = (ncol + cpw - 1) / cpw;
     int wpb = (int)((warps + sms - 1) / sms);
     wpb = wpb < 1 ? 1 : (wpb > 32 ? 32 : wpb);
     const int grid = (int)((warps + wpb - 1) / wpb);
+    ls.smem = present_smem_bytes(ncol, cfg->incols, cpw);
     int per_sm = 0;
     CK(present_max_blocks_per_sm(cpw, wpb * 32, ls.smem, &per_sm));
     if (per_sm >= 1 && grid <= per_sm * sms) {
