@@ -4,6 +4,6 @@ The product is ``_build/libaxon_b200.so`` (hand-written sm_100a CUDA behind the 
 ``include/axon_capi.h``) and the ``_build/axon`` command line that replaces the
 reference's ``build/axon``. This package is the Python side of the same C ABI.
 """
-from .network import CONFIG_C, Network, bstest, config, load_stim, stimuli  # noqa: F401
+from .network import CONFIG_C, Network, bstest, config, load_stim, multi_train, stimuli  # noqa: F401
 
-__all__ = ["Network", "config", "CONFIG_C", "stimuli", "load_stim", "bstest"]
+__all__ = ["Network", "config", "CONFIG_C", "stimuli", "load_stim", "bstest", "multi_train"]

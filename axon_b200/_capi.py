@@ -47,6 +47,29 @@ class StateDev(C.Structure):
     _fields_ = [(f, C.c_void_p) for f in STATE_DEV_FIELDS]
 
 
+MULTI_ARG_FIELDS = ["epochs", "T", "clamp_steps", "train_clamp", "stimcols", "wave_t", "readout", "autotune",
+                    "slots", "threads", "graph", "method"]
+
+
+class MultiArgs(C.Structure):
+    _fields_ = [(f, C.c_uint32) for f in MULTI_ARG_FIELDS] + [("reserved", C.c_uint32 * 4)]
+
+
+class MultiResult(C.Structure):
+    _fields_ = [("within_pct", C.c_double), ("recall", C.c_double), ("best_other", C.c_double),
+                ("drive_t6", C.c_double), ("wave_first", C.c_double), ("wave_last", C.c_double),
+                ("wdens_pct", C.c_double), ("steps", C.c_uint64)]
+
+
+class MultiReport(C.Structure):
+    _fields_ = [("gpu_ms", C.c_double), ("tune_ms", C.c_double), ("steps", C.c_uint64), ("train_steps", C.c_uint64),
+                ("slots", C.c_uint32), ("threads", C.c_uint32), ("tiles", C.c_uint32), ("grid", C.c_uint32),
+                ("graph", C.c_uint32), ("tried", C.c_uint32)]
+
+
+MULTI_ONE_LAUNCH, MULTI_PLAIN = 0, 1
+
+
 class AxonError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"axon status {status}: {msg}")
@@ -86,6 +109,8 @@ def lib() -> C.CDLL:
         L.axon_load_stim.argtypes = [U32P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, U32P]
         L.axon_present_static.argtypes = [C.POINTER(AxonCfg), C.POINTER(StateDev), C.c_uint32, C.c_uint32, C.c_int,
                                           C.c_uint32]
+        L.axon_multi_train.argtypes = [C.POINTER(C.c_void_p), C.c_uint32, U32P, U32P, C.POINTER(MultiArgs),
+                                       C.POINTER(MultiResult), C.POINTER(MultiReport)]
         for fn in (L.axon_recall, L.axon_recall_device):
             fn.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(RecallArgs), C.c_void_p, C.c_void_p,
                            C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]

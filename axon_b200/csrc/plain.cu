@@ -21,30 +21,11 @@
 
 #include "axon_device.cuh"
 #include "plain.cuh"
+#include "emit.cuh"
+#include "learn.cuh"
 #include "theta.cuh"
 
 namespace axon {
-
-// One 32-synapse word of k_learn's update, src/axon.mm:466-488: co-active pairs are
-// potentiated (phase 1), depressed ltdRep times (phase 2) or take the legacy rule
-// (phase 0); optional heterosynaptic LTD; then the clip band on every lane.
-__device__ __forceinline__ void learn_word(uint32_t& a0, uint32_t& a1, uint32_t& a2, uint32_t& a3, uint32_t sp,
-                                           bool want, uint32_t phase, uint32_t t, const PresentCfg& c,
-                                           uint32_t& nLTP, uint32_t& nLTD) {
-  const uint32_t co = want ? sp : 0u;
-  if (phase == 1u) {
-    bs_inc(a0, a1, a2, a3, co);
-    nLTP += __popc(co);
-  } else if (phase == 2u) {
-    for (uint32_t r = 0; r < c.ltdRep; ++r) bs_dec(a0, a1, a2, a3, co);
-    nLTD += __popc(co) * c.ltdRep;
-  } else {
-    bs_inc(a0, a1, a2, a3, co);
-    bs_dec(a0, a1, a2, a3, (want && (t % 2u == 1u)) ? ~sp : 0u);
-  }
-  if (c.hetero != 0u && phase == 1u) bs_dec(a0, a1, a2, a3, want ? ~sp : 0u);
-  if (c.bandHi != 0u) bs_clip(a0, a1, a2, a3, c.bandLo, c.bandHi);
-}
 
 template <int CPW>
 __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
@@ -173,32 +154,7 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
     const uint32_t gate = max(theta, 1u);
     cp_async_wait<0>();
     __syncthreads();
-    // k_emit gate and clamp (src/axon.mm:211-212), one presynaptic group of 8 columns per
-    // lane, with the group-activity bit of the next step's drive
-    for (uint32_t gb = warp * 32u; gb < ngrp; gb += wpb * 32u) {
-      const uint32_t g = gb + lane;
-      bool any = false;
-      if (g < ngrp) {
-        const uint4* d4 = reinterpret_cast<const uint4*>(sD) + 2 * g;
-        const uint4* b4 = reinterpret_cast<const uint4*>(sB) + 2 * g;
-        uint32_t w[8];
-        const uint4 d0 = d4[0], d1 = d4[1], b0 = b4[0], b1 = b4[1];
-        w[0] = d0.x < gate ? 0u : b0.x; w[1] = d0.y < gate ? 0u : b0.y;
-        w[2] = d0.z < gate ? 0u : b0.z; w[3] = d0.w < gate ? 0u : b0.w;
-        w[4] = d1.x < gate ? 0u : b1.x; w[5] = d1.y < gate ? 0u : b1.y;
-        w[6] = d1.z < gate ? 0u : b1.z; w[7] = d1.w < gate ? 0u : b1.w;
-        if (clamp && 8u * g < incols) {
-#pragma unroll
-          for (uint32_t k = 0; k < 8u; ++k)
-            if (8u * g + k < incols) w[k] = sStim[8u * g + k];
-        }
-        reinterpret_cast<uint4*>(sOut)[2 * g] = make_uint4(w[0], w[1], w[2], w[3]);
-        reinterpret_cast<uint4*>(sOut)[2 * g + 1] = make_uint4(w[4], w[5], w[6], w[7]);
-        any = (w[0] | w[1] | w[2] | w[3] | w[4] | w[5] | w[6] | w[7]) != 0u;
-      }
-      const uint32_t wv = __ballot_sync(kFull, any);
-      if (lane == 0) sActOut[gb >> 5] = wv;
-    }
+    emit_groups(sD, sB, sStim, sOut, sActOut, gate, clamp, incols, ngrp);
     __syncthreads();
     if (blockIdx.x == 0 && tid == 0) { d.theta[0] = theta; d.theta[1] = 0u; }
 

@@ -12,6 +12,7 @@
 #include <numeric>
 #include <stdexcept>
 
+#include "setops.hpp"
 #include "stimulus.hpp"
 
 namespace axon {
@@ -26,54 +27,6 @@ uint32_t argv_u32(int argc, char** argv, const char* key, uint32_t dflt) {
   for (int i = 1; i < argc; ++i)  // last occurrence wins (src/axon.mm:660-667)
     if (std::strncmp(argv[i], key, kl) == 0 && argv[i][kl] == '=') v = (uint32_t)std::atoi(argv[i] + kl + 1);
   return v;
-}
-
-using Ids = std::vector<uint32_t>;  // sorted column or neuron ids
-
-Ids active_columns(const uint32_t* spk, uint32_t incols, uint32_t ncol) {
-  Ids v;
-  for (uint32_t c = incols; c < ncol; ++c)
-    if (spk[c]) v.push_back(c);
-  return v;
-}
-Ids active_neurons(const uint32_t* spk, uint32_t incols, uint32_t ncol) {
-  Ids v;
-  for (uint32_t c = incols; c < ncol; ++c)
-    for (uint32_t b = spk[c]; b; b &= b - 1) v.push_back(c * kNpc + (uint32_t)__builtin_ctz(b));
-  return v;
-}
-size_t n_common(const Ids& a, const Ids& b) {
-  size_t i = 0, j = 0, k = 0;
-  while (i < a.size() && j < b.size()) {
-    if (a[i] < b[j]) ++i;
-    else if (b[j] < a[i]) ++j;
-    else { ++k; ++i; ++j; }
-  }
-  return k;
-}
-Ids common(const Ids& a, const Ids& b) {
-  Ids r;
-  std::set_intersection(a.begin(), a.end(), b.begin(), b.end(), std::back_inserter(r));
-  return r;
-}
-Ids minus(const Ids& a, const Ids& b) {
-  Ids r;
-  std::set_difference(a.begin(), a.end(), b.begin(), b.end(), std::back_inserter(r));
-  return r;
-}
-// cosine overlap |A n B| / sqrt(|A||B|), 0 for an empty set (src/axon.mm:896-901)
-double cos_overlap(const Ids& a, const Ids& b) {
-  if (a.empty() || b.empty()) return 0.0;
-  return (double)n_common(a, b) / std::sqrt((double)a.size() * b.size());
-}
-double jaccard(const Ids& a, const Ids& b) {
-  if (a.empty() || b.empty()) return 0.0;
-  const size_t i = n_common(a, b);
-  return (double)i / (double)(a.size() + b.size() - i);
-}
-void dedup(Ids& v) {
-  std::sort(v.begin(), v.end());
-  v.erase(std::unique(v.begin(), v.end()), v.end());
 }
 
 struct AxonFailure : std::runtime_error {

@@ -159,6 +159,32 @@ class Network:
         return out
 
 
+def multi_train(nets: list[Network], seeds: list[int], nstim: list[int], *, epochs: int, T: int = 10,
+                clamp_steps: int = 5, train_clamp: int | None = None, stimcols: int = 64, wave_t: int = 35,
+                readout: bool = True, autotune: bool = True, slots: int = 0, threads: int = 1024,
+                graph: bool = True, method: str = "launch") -> tuple[list[dict], dict]:
+    """The reference experiment for many networks at once (axon_multi_train).
+
+    Every network is initialised from its seed and trained on its own load; all
+    presentations run in one persistent launch (``method="launch"``) or through the plain
+    path, one launch per presentation (``method="plain"``). Returns the per-network
+    measurements and the launch report."""
+    n = len(nets)
+    assert len(seeds) == n and len(nstim) == n
+    a = A.MultiArgs(epochs=epochs, T=T, clamp_steps=clamp_steps,
+                    train_clamp=clamp_steps if train_clamp is None else train_clamp, stimcols=stimcols,
+                    wave_t=wave_t, readout=int(readout), autotune=int(autotune), slots=slots, threads=threads,
+                    graph=int(graph), method=A.MULTI_PLAIN if method == "plain" else A.MULTI_ONE_LAUNCH)
+    hs = (C.c_void_p * n)(*[x._h for x in nets])
+    sd = np.ascontiguousarray(seeds, dtype=np.uint32)
+    ns = np.ascontiguousarray(nstim, dtype=np.uint32)
+    res = (A.MultiResult * n)()
+    rep = A.MultiReport()
+    A.check(A.lib().axon_multi_train(hs, n, A.u32(sd), A.u32(ns), C.byref(a), res, C.byref(rep)))
+    out = [{f: getattr(r, f) for f, _ in A.MultiResult._fields_} for r in res]
+    return out, {f: getattr(rep, f) for f, _ in A.MultiReport._fields_}
+
+
 def stimuli(seed: int, nstim: int, incols: int, stimcols: int) -> np.ndarray:
     """Input patterns of the reference protocol (src/axon.mm:793-799), shape (nstim, stimcols)."""
     out = np.empty(nstim * stimcols, dtype=np.uint32)

@@ -188,6 +188,61 @@ typedef struct axon_state_dev {
 axon_status axon_present_static(const axon_cfg* cfg, const axon_state_dev* state, uint32_t T,
                                 uint32_t clamp_steps, int learn, uint32_t use_bias);
 
+/* ---------------------------------------------------------------- many networks, one launch
+ * The reference trains and reads out one network per process: build/axon runs init,
+ * epochs x nstim learning presentations plus one more of pattern 0 (src/axon.mm:1001-1033),
+ * then the readouts its measurements come from (src/axon.mm:1080-1105, 1495-1508,
+ * 1695-1730, 1804-1858). axon_multi_train runs that experiment for n networks at once:
+ * every network is initialised from seeds[i] with nstim[i] patterns (its load) and all
+ * their presentations run inside ONE persistent launch (captured as a CUDA graph when
+ * args->graph != 0), in slots of SMs that each take a queue of networks. The networks
+ * must share one axon_cfg and one device. With autotune != 0 the slot count and CTA shape
+ * are chosen by timing candidates on the networks themselves (they are re-initialised
+ * afterwards); networks are assigned to slots longest-first. method = 1 runs the same
+ * presentations through the plain path instead (one present launch each), for
+ * comparison. The ten settle presentations of src/axon.mm:1001 are not run: they change
+ * no weight or bias. With readout != 0, results[i] holds network i's measurements,
+ * computed as the reference's printing blocks compute them. */
+typedef struct axon_multi_args {
+  uint32_t epochs;      /* [epochs] */
+  uint32_t T;           /* [T] steps per presentation, 1..64 */
+  uint32_t clamp_steps; /* [clampsteps] cue steps of the readouts */
+  uint32_t train_clamp; /* [trainclamp] clamped steps of a learning presentation */
+  uint32_t stimcols;    /* [stimcols] columns per pattern */
+  uint32_t wave_t;      /* [wavet] steps of the wave readout (at most 60 are run) */
+  uint32_t readout;     /* 1: run the readouts and fill results */
+  uint32_t autotune;    /* 1: pick slots and CTA shape by timing candidates */
+  uint32_t slots;       /* autotune == 0: concurrent networks (0 = one per network, at most one per SM) */
+  uint32_t threads;     /* autotune == 0: 1024 (4 W3 tiles in flight per warp) or 512 (8 tiles) */
+  uint32_t graph;       /* 1: launch through a captured CUDA graph */
+  uint32_t method;      /* 0: one persistent launch, 1: plain path, one launch per presentation */
+  uint32_t reserved[4]; /* zero */
+} axon_multi_args;
+
+typedef struct axon_multi_result {
+  double within_pct; /* "within-assembly : ... = X%" (deep block) */
+  double recall;     /* 75% cue row: mean overlap with the own clamped reference */
+  double best_other; /* 75% cue row: mean best overlap with another reference */
+  double drive_t6;   /* "t6:" free-phase drive to assembly members */
+  double wave_first; /* wave ov(clampRef) at the first free step */
+  double wave_last;  /* wave ov(clampRef) at the last step (sustained = last / first, as printed) */
+  double wdens_pct;  /* functional synapse density after training, % */
+  uint64_t steps;    /* steps this network ran */
+} axon_multi_result;
+
+typedef struct axon_multi_report {
+  double gpu_ms;        /* device time of the training + readout launch (or of all plain launches) */
+  double tune_ms;       /* device time spent timing candidate shapes */
+  uint64_t steps;       /* network-steps run */
+  uint64_t train_steps; /* of which learning steps */
+  uint32_t slots, threads, tiles, grid; /* shape used (slots = 0 for the plain path) */
+  uint32_t graph;       /* 1 when the launch ran as a CUDA graph */
+  uint32_t tried;       /* candidate shapes timed */
+} axon_multi_report;
+
+axon_status axon_multi_train(axon_net* const* nets, uint32_t n, const uint32_t* seeds, const uint32_t* nstim,
+                             const axon_multi_args* args, axon_multi_result* results, axon_multi_report* report);
+
 /* Grid-wait limit of the persistent kernels in nanoseconds (default 2e9). */
 axon_status axon_set_wait_limit(axon_net* net, uint64_t ns);
 /* Text of the last error on this thread. */
