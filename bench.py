@@ -81,6 +81,48 @@ def events_per_step(hist: np.ndarray, conn: np.ndarray) -> np.ndarray:
     return ev
 
 
+MULTI_SEEDS, MULTI_LOADS = (0, 1, 2, 3, 4), (12, 24, 36, 48, 60)
+
+
+def printed(r: dict) -> dict:
+    """One network's measurements as the command line prints them."""
+    first, last = float(f"{r['wave_first']:.3f}"), float(f"{r['wave_last']:.3f}")
+    return {"within": f"{r['within_pct']:.2f}", "recall": f"{r['recall']:.3f}", "best_other": f"{r['best_other']:.3f}",
+            "margin": f"{r['recall'] - r['best_other']:+.3f}", "sustained": f"{last / first:.3f}",
+            "drive": f"{r['drive_t6']:.0f}"}
+
+
+def bench_multi(dev: int) -> dict:
+    """25 networks of uneven load (seeds 0-4 x loads 12..60, config C, 40 epochs plus the
+    readouts of the five measurements): one persistent launch with an autotuned shape,
+    against the plain path running the same presentations one launch each."""
+    import axon_b200 as ax
+
+    seeds = [s for s in MULTI_SEEDS for _ in MULTI_LOADS]
+    loads = [L for _ in MULTI_SEEDS for L in MULTI_LOADS]
+    nets = [ax.Network(config_c(), device=dev) for _ in seeds]
+    kw = dict(epochs=EPOCHS, T=10, clamp_steps=5, stimcols=STIMCOLS, wave_t=35)
+    try:
+        res_p, rep_p = ax.multi_train(nets, seeds, loads, method="plain", **kw)
+        res_m, rep_m = ax.multi_train(nets, seeds, loads, method="launch", autotune=True, graph=True, **kw)
+    finally:
+        for n in nets:
+            n.close()
+    assert res_m == res_p, "one-launch measurements differ from the plain path"
+    gold = {r["stim"]: {k: r[k] for k in ("within", "recall", "best_other", "margin", "sustained", "drive")}
+            for r in json.loads((ROOT / "tests" / "golden" / "published.json").read_text())["table1"]}
+    rows = {L: printed(res_m[i]) for i, (s, L) in enumerate(zip(seeds, loads)) if s == 0}
+    steps = rep_m["steps"]
+    return {"workload": "25 networks (seeds 0-4 x loads 12,24,36,48,60), config C, 40 epochs + readouts",
+            "networks": len(nets), "network_steps": steps, "learning_steps": rep_m["train_steps"],
+            "one_launch_ms": rep_m["gpu_ms"], "plain_ms": rep_p["gpu_ms"],
+            "one_launch_steps_per_s": steps / (rep_m["gpu_ms"] / 1e3),
+            "plain_steps_per_s": steps / (rep_p["gpu_ms"] / 1e3), "speedup_vs_plain": rep_p["gpu_ms"] / rep_m["gpu_ms"],
+            "shape": {k: rep_m[k] for k in ("slots", "threads", "tiles", "grid", "graph", "tried")},
+            "tune_ms": rep_m["tune_ms"], "bit_exact_vs_plain": True,
+            "seed0_rows": rows, "seed0_rows_equal_published_table1": all(rows[L] == gold[L] for L in rows)}
+
+
 def train(net, pats) -> float:
     import axon_b200 as ax
 
@@ -247,6 +289,7 @@ def main() -> None:
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
+    ap.add_argument("--no-multi", action="store_true", help="skip the 25-network one-launch measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -320,6 +363,8 @@ def main() -> None:
         pms = max_over_ranks(float(np.mean(pt)), dist)
         plain = {"value": world * events / (pms / 1e3), "ms_per_step": pms, "launches_per_step": B}
 
+    multi = None if args.no_multi else bench_multi(dev)
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -351,6 +396,7 @@ def main() -> None:
                 "d2h_bytes_per_step": int(B * NCOL * 4)},
         "plain": plain,
         "batched_over_plain": (value / plain["value"]) if plain else None,
+        "multi": multi,
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
     }
