@@ -70,6 +70,17 @@ class MultiReport(C.Structure):
 MULTI_ONE_LAUNCH, MULTI_PLAIN = 0, 1
 
 
+class ServeResult(C.Structure):
+    _fields_ = [("tag", C.c_uint64), ("net", C.c_uint32), ("steps", C.c_uint32), ("arrive_s", C.c_double),
+                ("admit_s", C.c_double), ("done_s", C.c_double)]
+
+
+class ServeCounters(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("in_flight", C.c_uint32), ("queued", C.c_uint64), ("ticks", C.c_uint64),
+                ("completed", C.c_uint64), ("max_batch", C.c_uint64), ("mean_batch", C.c_double),
+                ("busy_s", C.c_double)]
+
+
 class AxonError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"axon status {status}: {msg}")
@@ -111,6 +122,14 @@ def lib() -> C.CDLL:
                                           C.c_uint32]
         L.axon_multi_train.argtypes = [C.POINTER(C.c_void_p), C.c_uint32, U32P, U32P, C.POINTER(MultiArgs),
                                        C.POINTER(MultiResult), C.POINTER(MultiReport)]
+        L.axon_clock_s.restype = C.c_double
+        L.axon_serve_create.argtypes = [C.POINTER(C.c_void_p), C.c_uint32, C.c_uint64, C.POINTER(C.c_void_p)]
+        L.axon_serve_submit.argtypes = [C.c_void_p, C.c_uint32, U32P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                                        C.c_double]
+        L.axon_serve_poll.argtypes = [C.c_void_p, C.POINTER(ServeResult), U32P, C.c_uint32, C.POINTER(C.c_uint32)]
+        L.axon_serve_wait_idle.argtypes = [C.c_void_p, C.c_double]
+        L.axon_serve_stats.argtypes = [C.c_void_p, C.POINTER(ServeCounters)]
+        L.axon_serve_destroy.argtypes = [C.c_void_p]
         for fn in (L.axon_recall, L.axon_recall_device):
             fn.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(RecallArgs), C.c_void_p, C.c_void_p,
                            C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]

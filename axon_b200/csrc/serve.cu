@@ -1,0 +1,162 @@
+// Recall-serving tick: one readout step for every admitted trajectory.
+//
+// The step is k_drive + k_topk + k_emit of src/axon.mm:150-236 with learn = 0 (no bias, no
+// learning), exactly as the plain kernel runs a readout. Trajectories start and end at
+// any tick, so each carries its own local step: it reads spk(t-1) from its slot (all zero
+// at t = 0) and writes spk(t) into the other half of its ping-pong pair.
+//
+// k_serve_drive: a warp takes one (group of up to 8 trajectories of one network, column)
+// item. It loads each W3 tile that any member needs once and applies it to every member
+// whose presynaptic group is active, so the weights are read once per column per group
+// instead of once per trajectory; per member it forms the exact k-of-32 ballot and the
+// column drive.
+// k_serve_emit: a CTA per trajectory selects the column threshold over its drive vector
+// and rebuilds its spike vector and group-activity bits; a trajectory on its last step
+// also copies its final spikes to the done buffer.
+#include <cstdint>
+
+#include "axon_device.cuh"
+#include "emit.cuh"
+#include "serve.cuh"
+#include "theta.cuh"
+
+namespace axon {
+
+constexpr int kServeThreads = 256;
+
+__global__ void __launch_bounds__(kServeThreads) k_serve_drive(ServeDev d, ServeCfg c) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t ncol = c.ncol, ngroups = d.counts[1];
+  const uint64_t items = (uint64_t)ngroups * ncol;
+  for (uint64_t it = gwarp; it < items; it += nwarps) {
+    const uint32_t gi = (uint32_t)(it / ncol), cc = (uint32_t)(it % ncol);
+    const ServeGroup& G = d.grp[gi];
+    const ServeNet net = d.nets[G.net];
+    const uint32_t cn = __ldg(net.conn + cc * kNslot + lane);
+    const uint32_t n = G.n;
+    uint32_t actm[kServeGroup], acc[kServeGroup];
+    const uint32_t* spkIn[kServeGroup];
+    uint32_t uni = 0;
+#pragma unroll
+    for (int j = 0; j < (int)kServeGroup; ++j) {
+      actm[j] = 0u;
+      acc[j] = 0u;
+      spkIn[j] = nullptr;
+      if ((uint32_t)j < n) {
+        const ServeEntry e = d.ent[G.e[j]];
+        if (e.tloc > 0u) {  // spk(t-1) and its group-activity bits
+          const uint32_t* base = d.slots + (size_t)e.slot * d.slotWords;
+          const uint32_t par = (e.tloc - 1u) & 1u;
+          spkIn[j] = base + par * ncol;
+          const uint32_t* act = base + 2u * ncol + par * d.nactw;
+          actm[j] = __ballot_sync(kFull, (__ldcg(act + (cn >> 5)) >> (cn & 31u)) & 1u);
+        }
+      }
+      uni |= actm[j];
+    }
+    const uint4* Wt = net.W3 + (size_t)cc * kNslot * kTileU4 + lane;
+    while (uni) {
+      uint32_t s[4];
+      bool v[4];
+      uint4 w0[4], w1[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        v[u] = uni != 0u;
+        s[u] = v[u] ? (uint32_t)(__ffs(uni) - 1) : 0u;
+        uni &= uni - 1u;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (v[u]) {
+          w0[u] = __ldg(Wt + s[u] * kTileU4);
+          w1[u] = __ldg(Wt + s[u] * kTileU4 + 32);
+        }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (!v[u]) continue;
+        const uint32_t g = __shfl_sync(kFull, cn, s[u]);
+#pragma unroll
+        for (int j = 0; j < (int)kServeGroup; ++j) {
+          if (!((actm[j] >> s[u]) & 1u)) continue;  // warp-uniform
+          const uint4* sp = reinterpret_cast<const uint4*>(spkIn[j]);
+          const uint32_t cnt = popc4(w0[u], __ldcg(sp + 2 * g)) + popc4(w1[u], __ldcg(sp + 2 * g + 1));
+          const bool nmda = cnt >= c.dthr;
+          acc[j] += c.mode == 0u ? cnt : (c.mode == 1u ? (nmda ? cnt + c.boost : cnt) : (nmda ? 1u : 0u));
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < (int)kServeGroup; ++j) {
+      if ((uint32_t)j >= n) break;
+      uint32_t a = acc[j];
+      if (c.facil != 0u && spkIn[j] && ((__ldcg(spkIn[j] + cc) >> lane) & 1u)) a += c.facil;
+      const uint32_t drv = __reduce_add_sync(kFull, a);
+      uint32_t vk, vk1;
+      const uint32_t ball = warp_kwta(a, lane, c.k, vk, vk1);
+      if (lane == 0) {
+        uint32_t* base = d.slots + (size_t)d.ent[G.e[j]].slot * d.slotWords + 2u * ncol + 2u * d.nactw;
+        __stcg(base + cc, drv);          // xdrive
+        __stcg(base + ncol + cc, ball);  // xball
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kServeThreads) k_serve_emit(ServeDev d, ServeCfg c) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  const uint32_t ncol = c.ncol, incols = c.incols, ngrp = ncol / 8u;
+  uint32_t* sD = sm;
+  uint32_t* sStim = sD + ncol;
+  uint32_t* sHist = sStim + ((incols + 3u) & ~3u);
+  uint32_t* sRed = sHist + 256;
+  const uint32_t tid = threadIdx.x, nent = d.counts[0];
+  for (uint32_t ei = blockIdx.x; ei < nent; ei += gridDim.x) {
+    const ServeEntry e = d.ent[ei];
+    uint32_t* base = d.slots + (size_t)e.slot * d.slotWords;
+    const uint32_t* xdrive = base + 2u * ncol + 2u * d.nactw;
+    const uint32_t* xball = xdrive + ncol;
+    for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x)
+      cp_async16(reinterpret_cast<uint4*>(sD) + i, reinterpret_cast<const uint4*>(xdrive) + i);
+    cp_async_commit();
+    const bool clamp = e.tloc < e.clamp;
+    if (clamp) {  // clamp words of the cue (src/axon.mm:800-804: 0xFFFFFFFF on the cue's columns)
+      for (uint32_t i = tid; i < incols; i += blockDim.x) sStim[i] = 0u;
+      __syncthreads();
+      for (uint32_t i = tid; i < e.ncue; i += blockDim.x) {
+        const uint32_t col = d.cues[e.cueOff + i];
+        if (col < incols) sStim[col] = 0xFFFFFFFFu;
+      }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    const uint32_t theta = block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed, 0u);
+    uint32_t* spkOut = base + (e.tloc & 1u) * ncol;
+    uint32_t* actOut = base + 2u * ncol + (e.tloc & 1u) * d.nactw;
+    emit_groups(sD, xball, sStim, spkOut, actOut, max(theta, 1u), clamp, incols, ngrp);
+    if (e.done != 0xFFFFFFFFu) {
+      __syncthreads();
+      uint4* dst = reinterpret_cast<uint4*>(d.doneBuf + (size_t)e.done * ncol);
+      for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x) dst[i] = __ldcg(reinterpret_cast<const uint4*>(spkOut) + i);
+    }
+    __syncthreads();
+  }
+}
+
+size_t serve_emit_smem_bytes(uint32_t ncol, uint32_t incols) {
+  return ((size_t)ncol + ((incols + 3u) & ~3u) + 256 + 192) * 4;
+}
+
+cudaError_t serve_prepare(size_t emitSmem) {
+  return cudaFuncSetAttribute(k_serve_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)emitSmem);
+}
+
+cudaError_t launch_serve_tick(const ServeDev& d, const ServeCfg& c, int sms, size_t emitSmem, cudaStream_t st) {
+  k_serve_drive<<<sms * 8, kServeThreads, 0, st>>>(d, c);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_serve_emit<<<sms * 6, kServeThreads, emitSmem, st>>>(d, c);
+  return cudaGetLastError();
+}
+
+}  // namespace axon

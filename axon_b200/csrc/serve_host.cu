@@ -1,0 +1,392 @@
+// Recall server: continuous batching of readout trajectories over device-resident networks.
+//
+// The reference answers one readout at a time (present() with learn = 0,
+// src/axon.mm:815-888). The server accepts recall requests (network, cue columns, clamped
+// and free steps) at any time and runs them on an internal thread, tick by tick: at every
+// tick it admits requests that have arrived into free trajectory slots (the slot count is
+// set by the device-memory budget given at creation), advances every admitted trajectory
+// by one step in one batched pass (serve.cu), and retires the trajectories whose last step
+// ran, with their final spikes. A request's result does not depend on what else is in
+// flight: every trajectory reads only its own slot and the network's read-only weights.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "engine.hpp"
+#include "serve.cuh"
+
+using namespace axon;
+
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+size_t al(size_t bytes) { return (bytes + 255) & ~(size_t)255; }
+
+struct Request {
+  uint64_t tag = 0;
+  uint32_t net = 0, clamp = 0, steps = 0;
+  std::vector<uint32_t> cue;
+  double arrive = 0, admit = 0;
+};
+
+struct Active {
+  uint32_t slot;
+  uint32_t tloc;
+  Request req;
+};
+
+struct Done {
+  axon_serve_result r;
+  std::vector<uint32_t> spk;
+};
+
+}  // namespace
+
+struct axon_server {
+  std::vector<axon_net*> nets;
+  int device = 0, sms = 0;
+  uint32_t ncol = 0, incols = 0, nslots = 0;
+  ServeCfg cfg{};
+  size_t emitSmem = 0;
+  cudaStream_t stream = nullptr;
+  void* dmem = nullptr;        // slots, tables, done buffer
+  void* hmem = nullptr;        // pinned tick staging
+  void* hdone = nullptr;       // pinned done buffer
+  ServeDev dev{};
+  size_t stageBytes = 0;
+  std::vector<ServeEntry> entH;  // the tick's tables, built on the server thread
+  std::vector<ServeGroup> grpH;
+  std::vector<uint32_t> cueH;
+  std::vector<uint32_t> freeSlots;
+
+  std::mutex mu;
+  std::condition_variable cv, cvIdle;
+  std::deque<Request> queue;  // by arrival time
+  std::vector<Active> active;
+  std::deque<Done> done;
+  bool stop = false;
+  axon_status err = AXON_OK;
+  std::string errMsg;
+  std::thread th;
+  // statistics
+  uint64_t ticks = 0, sumActive = 0, maxActive = 0, completed = 0;
+  double busy = 0;
+
+  axon_status start(axon_net* const* ns, uint32_t n, uint64_t memBytes);
+  void loop();
+  axon_status tick();
+  void fail(axon_status s, const std::string& m) {
+    std::lock_guard<std::mutex> g(mu);
+    if (err == AXON_OK) { err = s; errMsg = m; }
+    cvIdle.notify_all();
+  }
+  ~axon_server();
+};
+
+#define CKS(call)                                                         \
+  do {                                                                    \
+    cudaError_t _e = (call);                                              \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call);                   \
+  } while (0)
+
+axon_status axon_server::start(axon_net* const* ns, uint32_t n, uint64_t memBytes) {
+  nets.assign(ns, ns + n);
+  axon_net* n0 = nets[0];
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!nets[i] || !nets[i]->initialized) return set_error(AXON_ESTATE, "serving needs initialised networks");
+    if (nets[i]->device != n0->device || nets[i]->ncol != n0->ncol || nets[i]->cfg.incols != n0->cfg.incols)
+      return set_error(AXON_EINVAL, "served networks must share device, ncol and incols");
+    if (std::memcmp(&nets[i]->cfg, &n0->cfg, sizeof(axon_cfg)) != 0)
+      return set_error(AXON_EINVAL, "served networks must share one configuration");
+  }
+  device = n0->device;
+  ncol = n0->ncol;
+  incols = n0->cfg.incols;
+  sms = n0->sm_count;
+  const PresentCfg pc = n0->present_cfg(1, 0, false, 0);  // readout parameters (learn = 0)
+  cfg.ncol = ncol; cfg.incols = incols; cfg.dthr = pc.dthr; cfg.boost = pc.boost; cfg.mode = pc.mode;
+  cfg.targetCols = pc.targetCols; cfg.k = pc.k; cfg.facil = pc.facil; cfg.topkPar = pc.topkPar;
+  CKS(cudaSetDevice(device));
+  // one slot: its buffers, its share of the done buffer and of the tick tables
+  const size_t slotBytes = (size_t)serve_slot_words(ncol) * 4;
+  const size_t perSlot = slotBytes + (size_t)ncol * 4 + sizeof(ServeEntry) + sizeof(ServeGroup) + (size_t)incols * 4;
+  const uint64_t fixed = al(n * sizeof(ServeNet)) + 4 * 256 + al(n * sizeof(ServeGroup));
+  if (memBytes <= fixed + perSlot) return set_error(AXON_EINVAL, "memory budget below one trajectory slot");
+  nslots = (uint32_t)std::min<uint64_t>((memBytes - fixed) / (perSlot + 64), 1u << 16);
+  stageBytes = 256 + al(nslots * sizeof(ServeEntry)) + al((nslots + n) * sizeof(ServeGroup)) +
+               al((size_t)nslots * incols * 4);
+  const size_t netsOff = 0, slotsOff = al(n * sizeof(ServeNet)), stageOff = slotsOff + al((size_t)nslots * slotBytes),
+               doneOff = stageOff + al(stageBytes), total = doneOff + al((size_t)nslots * ncol * 4);
+  if (cudaMalloc(&dmem, total) != cudaSuccess) {
+    cudaGetLastError();
+    dmem = nullptr;
+    return set_error(AXON_ENOMEM, "server device allocation failed");
+  }
+  CKS(cudaMallocHost(&hmem, stageBytes));
+  CKS(cudaMallocHost(&hdone, (size_t)nslots * ncol * 4));
+  CKS(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  char* b = (char*)dmem;
+  std::vector<ServeNet> hn(n);
+  for (uint32_t i = 0; i < n; ++i) hn[i] = ServeNet{nets[i]->d.W3, nets[i]->d.conn};
+  CKS(cudaMemcpyAsync(b + netsOff, hn.data(), n * sizeof(ServeNet), cudaMemcpyHostToDevice, stream));
+  dev.nets = (const ServeNet*)(b + netsOff);
+  dev.slots = (uint32_t*)(b + slotsOff);
+  dev.counts = (const uint32_t*)(b + stageOff);  // entries, groups and cues follow, packed per tick
+  dev.doneBuf = (uint32_t*)(b + doneOff);
+  dev.slotWords = serve_slot_words(ncol);
+  dev.nactw = serve_nactw(ncol);
+  emitSmem = serve_emit_smem_bytes(ncol, incols);
+  CKS(serve_prepare(emitSmem));
+  CKS(cudaStreamSynchronize(stream));
+  for (uint32_t s = nslots; s-- > 0;) freeSlots.push_back(s);
+  th = std::thread([this] { loop(); });
+  return AXON_OK;
+}
+
+axon_server::~axon_server() {
+  {
+    std::lock_guard<std::mutex> g(mu);
+    stop = true;
+  }
+  cv.notify_all();
+  if (th.joinable()) th.join();
+  if (stream) cudaStreamSynchronize(stream);
+  if (dmem) cudaFree(dmem);
+  if (hmem) cudaFreeHost(hmem);
+  if (hdone) cudaFreeHost(hdone);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void axon_server::loop() {
+  if (cudaSetDevice(device) != cudaSuccess) { fail(AXON_ECUDA, "cudaSetDevice in the server thread"); return; }
+  for (;;) {
+    {
+      std::unique_lock<std::mutex> g(mu);
+      for (;;) {
+        if (stop || err != AXON_OK) return;
+        if (!active.empty()) break;
+        if (!queue.empty()) {
+          const double wait = queue.front().arrive - now_s();
+          if (wait <= 0) break;
+          cv.wait_for(g, std::chrono::duration<double>(std::min(wait, 0.05)));
+        } else {
+          cvIdle.notify_all();
+          cv.wait_for(g, std::chrono::milliseconds(50));
+        }
+      }
+    }
+    const double t0 = now_s();
+    const axon_status s = tick();
+    if (s != AXON_OK) { fail(s, axon_last_error()); return; }
+    std::lock_guard<std::mutex> g(mu);
+    busy += now_s() - t0;
+  }
+}
+
+axon_status axon_server::tick() {
+  // admission: arrived requests, in arrival order, into free slots
+  std::vector<Active> admitted;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    const double t = now_s();
+    while (!queue.empty() && !freeSlots.empty() && queue.front().arrive <= t) {
+      Active a{freeSlots.back(), 0u, std::move(queue.front())};
+      freeSlots.pop_back();
+      queue.pop_front();
+      a.req.admit = t;
+      admitted.push_back(std::move(a));
+    }
+  }
+  for (auto& a : admitted) active.push_back(std::move(a));
+  if (active.empty()) return AXON_OK;
+  // the tick's tables: entries grouped by network, up to kServeGroup per group
+  std::sort(active.begin(), active.end(), [](const Active& x, const Active& y) {
+    return x.req.net != y.req.net ? x.req.net < y.req.net : x.slot < y.slot;
+  });
+  std::vector<ServeEntry>& ent = entH;
+  std::vector<ServeGroup>& grp = grpH;
+  std::vector<uint32_t>& cue = cueH;
+  ent.clear();
+  grp.clear();
+  cue.clear();
+  uint32_t ndone = 0;
+  for (const Active& a : active) {
+    ServeEntry e{};
+    e.slot = a.slot;
+    e.net = a.req.net;
+    e.tloc = a.tloc;
+    e.clamp = a.req.clamp;
+    if (a.tloc < a.req.clamp) {
+      e.ncue = (uint32_t)a.req.cue.size();
+      e.cueOff = (uint32_t)cue.size();
+      cue.insert(cue.end(), a.req.cue.begin(), a.req.cue.end());
+    }
+    e.done = (a.tloc + 1 == a.req.steps) ? ndone++ : 0xFFFFFFFFu;
+    if (grp.empty() || grp.back().net != e.net || grp.back().n == kServeGroup) {
+      ServeGroup g{};
+      g.net = e.net;
+      grp.push_back(g);
+    }
+    grp.back().e[grp.back().n++] = (uint32_t)ent.size();
+    ent.push_back(e);
+  }
+  const uint32_t ne = (uint32_t)ent.size(), ng = (uint32_t)grp.size(), nc = (uint32_t)cue.size();
+  // one upload: [counts][entries][groups][cue columns], packed to what this tick uses
+  const size_t oEnt = 256, oGrp = oEnt + al(ne * sizeof(ServeEntry)), oCue = oGrp + al(ng * sizeof(ServeGroup)),
+               bytes = oCue + (size_t)nc * 4;
+  char* h = (char*)hmem;
+  uint32_t* cnt = (uint32_t*)h;
+  cnt[0] = ne;
+  cnt[1] = ng;
+  std::memcpy(h + oEnt, ent.data(), ne * sizeof(ServeEntry));
+  std::memcpy(h + oGrp, grp.data(), ng * sizeof(ServeGroup));
+  if (nc) std::memcpy(h + oCue, cue.data(), (size_t)nc * 4);
+  ServeDev td = dev;
+  char* ds = (char*)dev.counts;
+  td.ent = (const ServeEntry*)(ds + oEnt);
+  td.grp = (const ServeGroup*)(ds + oGrp);
+  td.cues = (const uint32_t*)(ds + oCue);
+  CKS(cudaMemcpyAsync(ds, h, bytes, cudaMemcpyHostToDevice, stream));
+  CKS(launch_serve_tick(td, cfg, sms, emitSmem, stream));
+  if (ndone) CKS(cudaMemcpyAsync(hdone, dev.doneBuf, (size_t)ndone * ncol * 4, cudaMemcpyDeviceToHost, stream));
+  CKS(cudaStreamSynchronize(stream));
+  const double t = now_s();
+  // retire finished trajectories, advance the others
+  std::vector<Active> keep;
+  keep.reserve(active.size());
+  std::vector<Done> fin;
+  std::vector<uint32_t> freed;
+  for (uint32_t i = 0; i < ne; ++i) {
+    Active& a = active[i];
+    if (ent[i].done != 0xFFFFFFFFu) {
+      Done d;
+      d.r.tag = a.req.tag;
+      d.r.net = a.req.net;
+      d.r.steps = a.req.steps;
+      d.r.arrive_s = a.req.arrive;
+      d.r.admit_s = a.req.admit;
+      d.r.done_s = t;
+      const uint32_t* src = (const uint32_t*)hdone + (size_t)ent[i].done * ncol;
+      d.spk.assign(src, src + ncol);
+      fin.push_back(std::move(d));
+      freed.push_back(a.slot);
+    } else {
+      ++a.tloc;
+      keep.push_back(std::move(a));
+    }
+  }
+  active.swap(keep);
+  {
+    std::lock_guard<std::mutex> g(mu);
+    for (auto& d : fin) done.push_back(std::move(d));
+    for (uint32_t s : freed) freeSlots.push_back(s);
+    ++ticks;
+    sumActive += ne;
+    maxActive = std::max<uint64_t>(maxActive, ne);
+    completed += fin.size();
+    if (active.empty() && queue.empty()) cvIdle.notify_all();
+  }
+  return AXON_OK;
+}
+
+extern "C" {
+
+double axon_clock_s(void) { return now_s(); }
+
+axon_status axon_serve_create(axon_net* const* nets, uint32_t n, uint64_t mem_bytes, axon_server** out) {
+  if (!nets || !out || n == 0) return set_error(AXON_EINVAL, "null argument or n == 0");
+  *out = nullptr;
+  axon_server* s = new axon_server();
+  const axon_status st = s->start(nets, n, mem_bytes);
+  if (st != AXON_OK) {
+    delete s;
+    return st;
+  }
+  *out = s;
+  return AXON_OK;
+}
+
+axon_status axon_serve_submit(axon_server* s, uint32_t net, const uint32_t* cue_cols, uint32_t ncue,
+                              uint32_t clamp_steps, uint32_t free_steps, uint64_t tag, double arrive_s) {
+  if (!s || (ncue && !cue_cols)) return set_error(AXON_EINVAL, "null argument");
+  if (net >= s->nets.size()) return set_error(AXON_EINVAL, "network index out of range");
+  if (ncue > s->incols) return set_error(AXON_EINVAL, "more cue columns than input columns");
+  for (uint32_t i = 0; i < ncue; ++i)
+    if (cue_cols[i] >= s->incols) return set_error(AXON_EINVAL, "cue column outside the input columns");
+  if (clamp_steps + free_steps == 0) return set_error(AXON_EINVAL, "a request needs at least one step");
+  Request r;
+  r.tag = tag;
+  r.net = net;
+  r.clamp = clamp_steps;
+  r.steps = clamp_steps + free_steps;
+  r.cue.assign(cue_cols, cue_cols + ncue);
+  r.arrive = arrive_s > 0 ? arrive_s : now_s();
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->err != AXON_OK) return set_error(s->err, s->errMsg);
+    // keep the queue in arrival order (submissions normally come in order)
+    auto it = s->queue.end();
+    while (it != s->queue.begin() && (it - 1)->arrive > r.arrive) --it;
+    s->queue.insert(it, std::move(r));
+  }
+  s->cv.notify_all();
+  return AXON_OK;
+}
+
+axon_status axon_serve_poll(axon_server* s, axon_serve_result* res, uint32_t* final_spk, uint32_t max_results,
+                            uint32_t* n_out) {
+  if (!s || !n_out || (max_results && !res)) return set_error(AXON_EINVAL, "null argument");
+  std::lock_guard<std::mutex> g(s->mu);
+  uint32_t k = 0;
+  while (k < max_results && !s->done.empty()) {
+    Done& d = s->done.front();
+    res[k] = d.r;
+    if (final_spk) std::memcpy(final_spk + (size_t)k * s->ncol, d.spk.data(), (size_t)s->ncol * 4);
+    s->done.pop_front();
+    ++k;
+  }
+  *n_out = k;
+  if (s->err != AXON_OK) return set_error(s->err, s->errMsg);
+  return AXON_OK;
+}
+
+axon_status axon_serve_wait_idle(axon_server* s, double timeout_s) {
+  if (!s) return set_error(AXON_EINVAL, "null argument");
+  std::unique_lock<std::mutex> g(s->mu);
+  const auto until = std::chrono::steady_clock::now() + std::chrono::duration<double>(timeout_s);
+  while (s->err == AXON_OK && !(s->queue.empty() && s->freeSlots.size() == s->nslots)) {
+    if (s->cvIdle.wait_until(g, until) == std::cv_status::timeout) return set_error(AXON_ETIMEOUT, "server not idle in time");
+  }
+  if (s->err != AXON_OK) return set_error(s->err, s->errMsg);
+  return AXON_OK;
+}
+
+axon_status axon_serve_stats(axon_server* s, axon_serve_counters* out) {
+  if (!s || !out) return set_error(AXON_EINVAL, "null argument");
+  std::lock_guard<std::mutex> g(s->mu);
+  std::memset(out, 0, sizeof(*out));
+  out->slots = s->nslots;
+  out->ticks = s->ticks;
+  out->completed = s->completed;
+  out->mean_batch = s->ticks ? (double)s->sumActive / s->ticks : 0.0;
+  out->max_batch = s->maxActive;
+  out->busy_s = s->busy;
+  out->queued = s->queue.size();
+  out->in_flight = s->nslots - (uint32_t)s->freeSlots.size();
+  return AXON_OK;
+}
+
+axon_status axon_serve_destroy(axon_server* s) {
+  delete s;
+  return AXON_OK;
+}
+
+}  // extern "C"

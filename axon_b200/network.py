@@ -185,6 +185,70 @@ def multi_train(nets: list[Network], seeds: list[int], nstim: list[int], *, epoc
     return out, {f: getattr(rep, f) for f, _ in A.MultiReport._fields_}
 
 
+def clock_s() -> float:
+    """The monotonic host clock the server stamps requests with (seconds)."""
+    return float(A.lib().axon_clock_s())
+
+
+class Server:
+    """Recall server over device-resident networks (axon_serve_*): requests are readout
+    trajectories (cue columns clamped for ``clamp_steps``, then ``free_steps`` free steps)
+    run with continuous batching on an internal thread of the library."""
+
+    def __init__(self, nets: list[Network], mem_bytes: int = 64 << 20):
+        self.nets = list(nets)
+        self.ncol = nets[0].ncol
+        hs = (C.c_void_p * len(nets))(*[x._h for x in nets])
+        h = C.c_void_p()
+        A.check(A.lib().axon_serve_create(hs, len(nets), mem_bytes, C.byref(h)))
+        self._h = h
+
+    def submit(self, net: int, cue_cols, clamp_steps: int, free_steps: int, tag: int, arrive_s: float = 0.0) -> None:
+        cols = np.ascontiguousarray(cue_cols, dtype=np.uint32)
+        A.check(A.lib().axon_serve_submit(self._h, net, A.u32(cols) if cols.size else None, cols.size, clamp_steps,
+                                          free_steps, tag, arrive_s))
+
+    def poll(self, max_results: int = 4096, spikes: bool = True) -> list[tuple[dict, np.ndarray | None]]:
+        res = (A.ServeResult * max_results)()
+        spk = np.empty((max_results, self.ncol), dtype=np.uint32) if spikes else None
+        n = C.c_uint32()
+        A.check(A.lib().axon_serve_poll(self._h, res, A.u32(spk) if spikes else None, max_results, C.byref(n)))
+        return [({f: getattr(res[i], f) for f, _ in A.ServeResult._fields_}, spk[i].copy() if spikes else None)
+                for i in range(n.value)]
+
+    def wait_idle(self, timeout_s: float = 120.0) -> None:
+        A.check(A.lib().axon_serve_wait_idle(self._h, timeout_s))
+
+    def stats(self) -> dict:
+        c = A.ServeCounters()
+        A.check(A.lib().axon_serve_stats(self._h, C.byref(c)))
+        return {f: getattr(c, f) for f, _ in A.ServeCounters._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            A.lib().axon_serve_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def clamp_words(cols, ncol: int) -> np.ndarray:
+    """Clamp words with 0xFFFFFFFF on the given input columns (the reference's clamp form)."""
+    w = np.zeros(ncol, dtype=np.uint32)
+    w[np.asarray(cols, dtype=np.int64)] = 0xFFFFFFFF
+    return w
+
+
 def stimuli(seed: int, nstim: int, incols: int, stimcols: int) -> np.ndarray:
     """Input patterns of the reference protocol (src/axon.mm:793-799), shape (nstim, stimcols)."""
     out = np.empty(nstim * stimcols, dtype=np.uint32)

@@ -123,6 +123,87 @@ def bench_multi(dev: int) -> dict:
             "seed0_rows": rows, "seed0_rows_equal_published_table1": all(rows[L] == gold[L] for L in rows)}
 
 
+SERVE_LOADS = (12, 36, 60, 100, 140, 170, 200, 200)
+SERVE_RATES = (2000, 10000, 50000)
+SERVE_SECONDS = 1.0
+
+
+def bench_serve(dev: int) -> dict:
+    """Recall serving: 8 trained networks (config C, loads 12..200, seeds 0-7) answer
+    Poisson-arriving recall requests (cue = 16-64 of a stored pattern's columns, 5 clamped
+    + 10-60 free steps) with continuous batching; latency = result on the host - arrival."""
+    import axon_b200 as ax
+
+    seeds = list(range(len(SERVE_LOADS)))
+    nets = [ax.Network(config_c(), device=dev) for _ in seeds]
+    try:
+        _, rep = ax.multi_train(nets, seeds, list(SERVE_LOADS), epochs=EPOCHS, T=10, clamp_steps=5, stimcols=STIMCOLS,
+                                readout=False, autotune=True)
+        pats = [ax.stimuli(sd, L, INCOLS, STIMCOLS) for sd, L in zip(seeds, SERVE_LOADS)]
+        refs = []  # clamped reference assemblies (active recurrent columns per pattern)
+        for net, P in zip(nets, pats):
+            cues = np.stack([ax.load_stim(P[q], 1.0, 2000 + q, NCOL) for q in range(len(P))])
+            fin = net.recall(cues, 10, 10)["final"]
+            refs.append([set(np.nonzero(fin[q, INCOLS:])[0].tolist()) for q in range(len(P))])
+        out = {"workload": "8 networks (config C, loads 12,36,60,100,140,170,200,200, seeds 0-7); Poisson arrivals; "
+                           "cue 16-64 columns of a stored pattern; 5 clamped + 10-60 free steps",
+               "train_ms": rep["gpu_ms"], "rates": []}
+        srv = ax.Server(nets, 256 << 20)
+        try:
+            out["slots"] = srv.stats()["slots"]
+            rng = np.random.default_rng(12345)
+            tag = 0
+            for rate in SERVE_RATES:
+                n = int(rate * SERVE_SECONDS)
+                gaps = rng.exponential(1.0 / rate, n)
+                reqs = []
+                for i in range(n):
+                    net = int(rng.integers(len(nets)))
+                    q = int(rng.integers(len(pats[net])))
+                    size = int(rng.integers(16, 65))
+                    cols = np.sort(rng.choice(pats[net][q], size, replace=False)).astype(np.uint32)
+                    reqs.append((tag + i, net, q, cols, int(rng.integers(10, 61))))
+                t0 = ax.clock_s() + 0.3
+                arrive = t0 + np.cumsum(gaps)
+                for (tg, net, q, cols, free), a in zip(reqs, arrive):
+                    srv.submit(net, cols, 5, free, tg, float(a))
+                sample = {r[0]: r for r in reqs[:: max(1, n // 16)]}
+                lat, ov, first, last, got, exact = [], [], None, 0.0, 0, True
+                info = {r[0]: r for r in reqs}
+                while got < n:
+                    done = srv.poll(4096)
+                    if not done:
+                        time.sleep(0.002)
+                        continue
+                    for res, spk in done:
+                        _, net, q, cols, free = info[res["tag"]]
+                        lat.append(res["done_s"] - res["arrive_s"])
+                        last = max(last, res["done_s"])
+                        act = set(np.nonzero(spk[INCOLS:])[0].tolist())
+                        ref = refs[net][q]
+                        ov.append(len(act & ref) / np.sqrt(len(act) * len(ref)) if act and ref else 0.0)
+                        if res["tag"] in sample:
+                            alone = nets[net].recall(ax.clamp_words(cols, NCOL)[None, :], 5 + free, 5,
+                                                     method="plain")["final"][0]
+                            exact &= bool(np.array_equal(alone, spk))
+                    got += len(done)
+                st = srv.stats()
+                lat_ms = np.array(lat) * 1e3
+                out["rates"].append({"offered_req_s": rate, "requests": n,
+                                     "trajectories_per_s": n / (last - float(arrive[0])),
+                                     "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+                                     "mean_overlap_with_reference": float(np.mean(ov)),
+                                     "sample_bit_exact_vs_alone": exact, "sample": len(sample),
+                                     "mean_batch_so_far": st["mean_batch"], "max_batch_so_far": st["max_batch"]})
+                tag += n
+        finally:
+            srv.close()
+    finally:
+        for x in nets:
+            x.close()
+    return out
+
+
 def train(net, pats) -> float:
     import axon_b200 as ax
 
@@ -290,6 +371,7 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
     ap.add_argument("--no-multi", action="store_true", help="skip the 25-network one-launch measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the recall-serving measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -364,6 +446,7 @@ def main() -> None:
         plain = {"value": world * events / (pms / 1e3), "ms_per_step": pms, "launches_per_step": B}
 
     multi = None if args.no_multi else bench_multi(dev)
+    serving = None if args.no_serve else bench_serve(dev)
 
     if rank != 0:
         if dist is not None:
@@ -397,6 +480,7 @@ def main() -> None:
         "plain": plain,
         "batched_over_plain": (value / plain["value"]) if plain else None,
         "multi": multi,
+        "serving": serving,
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
     }

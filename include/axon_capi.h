@@ -243,6 +243,56 @@ typedef struct axon_multi_report {
 axon_status axon_multi_train(axon_net* const* nets, uint32_t n, const uint32_t* seeds, const uint32_t* nstim,
                              const axon_multi_args* args, axon_multi_result* results, axon_multi_report* report);
 
+/* ---------------------------------------------------------------- recall serving
+ * The reference runs one readout at a time: present() with learn = 0 (src/axon.mm:815-888),
+ * the clamp built from a pattern's kept columns (src/axon.mm:800-804). A server answers
+ * such readouts as requests against device-resident trained networks, with continuous
+ * batching: an internal thread advances, tick by tick, every admitted trajectory by one
+ * step in one batched pass (trajectories of one network share each weight-tile load),
+ * admits requests that have arrived into slots as they free up (the slot count follows
+ * from mem_bytes, the device memory the server may use), and retires finished ones. A
+ * request's final spikes are the same as those of axon_recall for the same network, cue
+ * and steps, whatever else is in flight. The networks must share one axon_cfg and device
+ * and must not be changed (present, write, init) while the server exists.
+ * Times are seconds of axon_clock_s(), a monotonic host clock. */
+typedef struct axon_server axon_server;
+
+typedef struct axon_serve_result {
+  uint64_t tag;    /* the caller's request id */
+  uint32_t net;    /* network index */
+  uint32_t steps;  /* clamped + free steps run */
+  double arrive_s; /* arrival time given at submission */
+  double admit_s;  /* time the request got a slot */
+  double done_s;   /* time its final spikes reached the host */
+} axon_serve_result;
+
+typedef struct axon_serve_counters {
+  uint32_t slots;      /* trajectory slots the memory budget allows */
+  uint32_t in_flight;  /* slots in use now */
+  uint64_t queued;     /* submitted, not yet admitted */
+  uint64_t ticks;      /* batched steps run */
+  uint64_t completed;  /* requests finished */
+  uint64_t max_batch;  /* most trajectories advanced in one tick */
+  double mean_batch;   /* trajectories per tick, mean */
+  double busy_s;       /* time spent in ticks */
+} axon_serve_counters;
+
+double axon_clock_s(void);
+axon_status axon_serve_create(axon_net* const* nets, uint32_t n, uint64_t mem_bytes, axon_server** out);
+/* cue_cols: the ncue input columns clamped on (each < incols); the trajectory runs
+ * clamp_steps clamped then free_steps free steps. arrive_s: arrival time (0 = now); a
+ * request is not admitted before it. Latency = done_s - arrive_s. */
+axon_status axon_serve_submit(axon_server* s, uint32_t net, const uint32_t* cue_cols, uint32_t ncue,
+                              uint32_t clamp_steps, uint32_t free_steps, uint64_t tag, double arrive_s);
+/* Up to max_results finished requests, oldest first; final_spk (NULL to skip) receives
+ * ncol words per result. */
+axon_status axon_serve_poll(axon_server* s, axon_serve_result* res, uint32_t* final_spk, uint32_t max_results,
+                            uint32_t* n_out);
+/* Blocks until nothing is queued or in flight (AXON_ETIMEOUT after timeout_s). */
+axon_status axon_serve_wait_idle(axon_server* s, double timeout_s);
+axon_status axon_serve_stats(axon_server* s, axon_serve_counters* out);
+axon_status axon_serve_destroy(axon_server* s);
+
 /* Grid-wait limit of the persistent kernels in nanoseconds (default 2e9). */
 axon_status axon_set_wait_limit(axon_net* net, uint64_t ns);
 /* Text of the last error on this thread. */
