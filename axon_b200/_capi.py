@@ -78,7 +78,7 @@ class ServeResult(C.Structure):
 class ServeCounters(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("in_flight", C.c_uint32), ("queued", C.c_uint64), ("ticks", C.c_uint64),
                 ("completed", C.c_uint64), ("max_batch", C.c_uint64), ("mean_batch", C.c_double),
-                ("busy_s", C.c_double)]
+                ("busy_s", C.c_double), ("drive_s", C.c_double), ("emit_s", C.c_double)]
 
 
 class AxonError(RuntimeError):
@@ -116,6 +116,7 @@ def lib() -> C.CDLL:
         L.axon_bstest.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, U32P, U32P, U32P, U32P, U32P,
                                   C.c_uint64]
         L.axon_set_wait_limit.argtypes = [C.c_void_p, C.c_uint64]
+        L.axon_inject_missing_arrival.argtypes = [C.c_void_p, C.c_uint32]
         L.axon_stimuli.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, U32P]
         L.axon_load_stim.argtypes = [U32P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, U32P]
         L.axon_present_static.argtypes = [C.POINTER(AxonCfg), C.POINTER(StateDev), C.c_uint32, C.c_uint32, C.c_int,

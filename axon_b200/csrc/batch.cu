@@ -91,6 +91,7 @@ __device__ __forceinline__ uint32_t branch_term(uint32_t cnt, uint32_t dthr, uin
 }
 
 constexpr uint32_t kColWords = kNslot * 256;             // one column's 32 tiles
+constexpr uint64_t kDrainNs = 1000000000ull;             // bound on waiting for own copies after a timeout
 constexpr uint32_t kItemWords = kRecallCpi * kColWords;  // one work item
 
 template <bool PACK>
@@ -205,11 +206,19 @@ __global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
         P[33 + lane] = tot0 + i1;
         if (lane == 0) P[0] = 0u;
       }
-      const bool ok = mbar_wait(&sBar[bcur], (bcur ? uses1 : uses0) & 1u, c.waitNs);
+      const uint32_t parCur = (bcur ? uses1 : uses0) & 1u;
+      const bool ok = mbar_wait(&sBar[bcur], parCur, c.waitNs);
       if (bcur) ++uses1; else ++uses0;
       if (__syncthreads_or(!ok)) {
-        if (tid == 0) atomicCAS(d.err, 0u, kErrTimeout);
-        mbar_wait(&sBar[bcur ^ 1u], (bcur ? uses0 : uses1) & 1u, c.waitNs);  // copies still in flight
+        if (tid == 0) {
+          atomicCAS(d.err, 0u, kErrTimeout);
+          // the copies this CTA issued must land before its shared memory is released:
+          // wait for both buffers' outstanding copies, with a bound of its own
+          const uint64_t drain = c.waitNs > kDrainNs ? c.waitNs : kDrainNs;
+          mbar_wait(&sBar[bcur], parCur, drain);
+          if (sMisc[2] < nitems) mbar_wait(&sBar[bcur ^ 1u], (bcur ? uses0 : uses1) & 1u, drain);
+        }
+        __syncthreads();
         return;
       }
       const uint32_t E1 = sP1[64], E = E1 + sPM[64], units = (E + 31u) >> 5;

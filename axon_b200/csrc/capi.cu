@@ -142,6 +142,12 @@ axon_status axon_set_wait_limit(axon_net* net, uint64_t ns) {
   return AXON_OK;
 }
 
+axon_status axon_inject_missing_arrival(axon_net* net, uint32_t missing) {
+  if (!net || missing == 0 || missing > 1024) return fail(AXON_EINVAL, "bad argument");
+  net->inject_missing = missing;
+  return AXON_OK;
+}
+
 axon_status axon_stimuli(uint32_t seed, uint32_t nstim, uint32_t incols, uint32_t stimcols, uint32_t* out) {
   if (!out || stimcols > incols) return fail(AXON_EINVAL, "bad argument");
   const auto pats = make_patterns(seed, nstim, incols, stimcols);

@@ -191,7 +191,9 @@ axon_status axon_net::present(const uint32_t* stim, uint32_t T, uint32_t clampSt
   CK(cudaMemcpyAsync(d.stim, hstim, (size_t)ncol * 4, cudaMemcpyHostToDevice, stream));
   CK(cudaMemsetAsync(d.stats, 0, 1024 * 4, stream));
   CK(cudaMemsetAsync(d.bar, 0, 4, stream));
-  const PresentCfg pc = present_cfg(T, clampSteps, learn, useBias);
+  PresentCfg pc = present_cfg(T, clampSteps, learn, useBias);
+  pc.missing = inject_missing;
+  inject_missing = 0;
   if (learn) w3b_valid = false;
   CK(cudaEventRecord(ev0, stream));
   CK(launch_present(d, pc, shape, stream));

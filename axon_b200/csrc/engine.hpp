@@ -41,6 +41,7 @@ struct axon_net {
   axon::LaunchShape shape{};
   bool initialized = false;
   uint64_t wait_ns = 2000000000ull;
+  uint32_t inject_missing = 0;  // one-shot: the next persistent launch waits for this many absent CTAs
 
   axon_status create(const axon_cfg& c, int dev);
   void release();

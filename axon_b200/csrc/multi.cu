@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(NT, 1) k_multi(MultiDev m, MultiCfg c) {
           }
         }
 
-        if (!grid_barrier(bar, m.err, nb, gstep, c.waitNs, sFlag)) return;
+        if (!grid_barrier(bar, m.err, nb + c.missing, gstep, c.waitNs, sFlag)) return;
 
         // ---------------- phase B: column threshold (k_topk) and the full spike vector
         {

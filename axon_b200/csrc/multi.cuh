@@ -48,8 +48,8 @@ struct MultiDev {
 struct MultiCfg {
   uint32_t ncol, incols, dthr, boost, mode, targetCols, biasUp, biasDown, biasShift, biasDownEvery, bandLo, bandHi,
       marginGate, hetero, ltdRep, contrast, ltdEvery, topkPar;
-  uint32_t maxCpw;  // largest columns-per-warp of any slot (sizes the shared memory)
-  uint32_t pad;
+  uint32_t maxCpw;   // largest columns-per-warp of any slot (sizes the shared memory)
+  uint32_t missing;  // CTAs every slot barrier waits for beyond the slot: 0, or more to test failure detection
   uint64_t waitNs;
 };
 

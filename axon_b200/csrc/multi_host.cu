@@ -535,6 +535,8 @@ axon_status MultiRun::run(const uint32_t* seeds, const uint32_t* nstim, axon_mul
   cfg_.biasDownEvery = pc.biasDownEvery; cfg_.bandLo = pc.bandLo; cfg_.bandHi = pc.bandHi;
   cfg_.marginGate = pc.marginGate; cfg_.hetero = pc.hetero; cfg_.ltdRep = pc.ltdRep; cfg_.contrast = pc.contrast;
   cfg_.ltdEvery = pc.ltdEvery; cfg_.topkPar = pc.topkPar; cfg_.waitNs = net0_->wait_ns;
+  cfg_.missing = net0_->inject_missing;
+  net0_->inject_missing = 0;
 
   axon_status st = plan(seeds, nstim);
   if (st != AXON_OK) return st;

@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
       }
     }
 
-    if (!grid_barrier(d.bar, d.err, gridDim.x, t, c.waitNs, sFlag)) return;
+    if (!grid_barrier(d.bar, d.err, gridDim.x + c.missing, t, c.waitNs, sFlag)) return;
 
     // ---------------- phase B: column threshold (k_topk) and the full spike vector
     // drives and ballots come from L2 by asynchronous copies; the ballots keep arriving

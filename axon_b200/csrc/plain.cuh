@@ -21,6 +21,7 @@ struct NetDev {
 struct PresentCfg {
   uint32_t ncol, incols, T, clampSteps, learn, k, dthr, boost, mode, targetCols, useBias, facil, biasUp, biasDown,
       biasShift, biasDownEvery, bandLo, bandHi, marginGate, hetero, ltdRep, contrast, ltdEvery, topkPar;
+  uint32_t missing;  // CTAs every grid barrier waits for beyond the launch: 0, or more to test failure detection
   uint64_t waitNs;
 };
 

@@ -24,7 +24,9 @@ namespace axon {
 
 constexpr int kServeThreads = 256;
 
-__global__ void __launch_bounds__(kServeThreads) k_serve_drive(ServeDev d, ServeCfg c) {
+// Spike vectors and activity bits were written by the previous tick's emit kernel and are
+// read-only here, so they are read through the non-coherent L1 path.
+__global__ void __launch_bounds__(kServeThreads, 3) k_serve_drive(ServeDev d, ServeCfg c) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t ncol = c.ncol, ngroups = d.counts[1];
@@ -50,7 +52,7 @@ __global__ void __launch_bounds__(kServeThreads) k_serve_drive(ServeDev d, Serve
           const uint32_t par = (e.tloc - 1u) & 1u;
           spkIn[j] = base + par * ncol;
           const uint32_t* act = base + 2u * ncol + par * d.nactw;
-          actm[j] = __ballot_sync(kFull, (__ldcg(act + (cn >> 5)) >> (cn & 31u)) & 1u);
+          actm[j] = __ballot_sync(kFull, (__ldg(act + (cn >> 5)) >> (cn & 31u)) & 1u);
         }
       }
       uni |= actm[j];
@@ -80,7 +82,7 @@ __global__ void __launch_bounds__(kServeThreads) k_serve_drive(ServeDev d, Serve
         for (int j = 0; j < (int)kServeGroup; ++j) {
           if (!((actm[j] >> s[u]) & 1u)) continue;  // warp-uniform
           const uint4* sp = reinterpret_cast<const uint4*>(spkIn[j]);
-          const uint32_t cnt = popc4(w0[u], __ldcg(sp + 2 * g)) + popc4(w1[u], __ldcg(sp + 2 * g + 1));
+          const uint32_t cnt = popc4(w0[u], __ldg(sp + 2 * g)) + popc4(w1[u], __ldg(sp + 2 * g + 1));
           const bool nmda = cnt >= c.dthr;
           acc[j] += c.mode == 0u ? cnt : (c.mode == 1u ? (nmda ? cnt + c.boost : cnt) : (nmda ? 1u : 0u));
         }
@@ -90,7 +92,7 @@ __global__ void __launch_bounds__(kServeThreads) k_serve_drive(ServeDev d, Serve
     for (int j = 0; j < (int)kServeGroup; ++j) {
       if ((uint32_t)j >= n) break;
       uint32_t a = acc[j];
-      if (c.facil != 0u && spkIn[j] && ((__ldcg(spkIn[j] + cc) >> lane) & 1u)) a += c.facil;
+      if (c.facil != 0u && spkIn[j] && ((__ldg(spkIn[j] + cc) >> lane) & 1u)) a += c.facil;
       const uint32_t drv = __reduce_add_sync(kFull, a);
       uint32_t vk, vk1;
       const uint32_t ball = warp_kwta(a, lane, c.k, vk, vk1);
@@ -151,9 +153,11 @@ cudaError_t serve_prepare(size_t emitSmem) {
   return cudaFuncSetAttribute(k_serve_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)emitSmem);
 }
 
-cudaError_t launch_serve_tick(const ServeDev& d, const ServeCfg& c, int sms, size_t emitSmem, cudaStream_t st) {
+cudaError_t launch_serve_tick(const ServeDev& d, const ServeCfg& c, int sms, size_t emitSmem, cudaStream_t st,
+                              cudaEvent_t between) {
   k_serve_drive<<<sms * 8, kServeThreads, 0, st>>>(d, c);
   cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && between) e = cudaEventRecord(between, st);
   if (e != cudaSuccess) return e;
   k_serve_emit<<<sms * 6, kServeThreads, emitSmem, st>>>(d, c);
   return cudaGetLastError();

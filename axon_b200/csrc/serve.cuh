@@ -60,6 +60,8 @@ inline uint32_t serve_nactw(uint32_t ncol) { return ((((ncol / 8u) + 31u) / 32u)
 
 size_t serve_emit_smem_bytes(uint32_t ncol, uint32_t incols);
 cudaError_t serve_prepare(size_t emitSmem);
-cudaError_t launch_serve_tick(const ServeDev& d, const ServeCfg& c, int sms, size_t emitSmem, cudaStream_t st);
+// the two kernels of one tick; `between` (may be null) is recorded after the first
+cudaError_t launch_serve_tick(const ServeDev& d, const ServeCfg& c, int sms, size_t emitSmem, cudaStream_t st,
+                              cudaEvent_t between);
 
 }  // namespace axon

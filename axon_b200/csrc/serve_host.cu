@@ -78,7 +78,8 @@ struct axon_server {
   std::thread th;
   // statistics
   uint64_t ticks = 0, sumActive = 0, maxActive = 0, completed = 0;
-  double busy = 0;
+  double busy = 0, driveS = 0, emitS = 0;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
 
   axon_status start(axon_net* const* ns, uint32_t n, uint64_t memBytes);
   void loop();
@@ -133,6 +134,7 @@ axon_status axon_server::start(axon_net* const* ns, uint32_t n, uint64_t memByte
   CKS(cudaMallocHost(&hmem, stageBytes));
   CKS(cudaMallocHost(&hdone, (size_t)nslots * ncol * 4));
   CKS(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  for (auto& e : ev) CKS(cudaEventCreate(&e));
   char* b = (char*)dmem;
   std::vector<ServeNet> hn(n);
   for (uint32_t i = 0; i < n; ++i) hn[i] = ServeNet{nets[i]->d.W3, nets[i]->d.conn};
@@ -162,6 +164,8 @@ axon_server::~axon_server() {
   if (dmem) cudaFree(dmem);
   if (hmem) cudaFreeHost(hmem);
   if (hdone) cudaFreeHost(hdone);
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -255,10 +259,15 @@ axon_status axon_server::tick() {
   td.grp = (const ServeGroup*)(ds + oGrp);
   td.cues = (const uint32_t*)(ds + oCue);
   CKS(cudaMemcpyAsync(ds, h, bytes, cudaMemcpyHostToDevice, stream));
-  CKS(launch_serve_tick(td, cfg, sms, emitSmem, stream));
+  CKS(cudaEventRecord(ev[0], stream));
+  CKS(launch_serve_tick(td, cfg, sms, emitSmem, stream, ev[1]));
+  CKS(cudaEventRecord(ev[2], stream));
   if (ndone) CKS(cudaMemcpyAsync(hdone, dev.doneBuf, (size_t)ndone * ncol * 4, cudaMemcpyDeviceToHost, stream));
   CKS(cudaStreamSynchronize(stream));
   const double t = now_s();
+  float msDrive = 0.f, msEmit = 0.f;
+  CKS(cudaEventElapsedTime(&msDrive, ev[0], ev[1]));
+  CKS(cudaEventElapsedTime(&msEmit, ev[1], ev[2]));
   // retire finished trajectories, advance the others
   std::vector<Active> keep;
   keep.reserve(active.size());
@@ -289,6 +298,8 @@ axon_status axon_server::tick() {
     for (auto& d : fin) done.push_back(std::move(d));
     for (uint32_t s : freed) freeSlots.push_back(s);
     ++ticks;
+    driveS += msDrive * 1e-3;
+    emitS += msEmit * 1e-3;
     sumActive += ne;
     maxActive = std::max<uint64_t>(maxActive, ne);
     completed += fin.size();
@@ -379,6 +390,8 @@ axon_status axon_serve_stats(axon_server* s, axon_serve_counters* out) {
   out->mean_batch = s->ticks ? (double)s->sumActive / s->ticks : 0.0;
   out->max_batch = s->maxActive;
   out->busy_s = s->busy;
+  out->drive_s = s->driveS;
+  out->emit_s = s->emitS;
   out->queued = s->queue.size();
   out->in_flight = s->nslots - (uint32_t)s->freeSlots.size();
   return AXON_OK;

@@ -68,6 +68,10 @@ class Network:
     def set_wait_limit(self, ns: int) -> None:
         A.check(A.lib().axon_set_wait_limit(self._h, ns))
 
+    def inject_missing_arrival(self, missing: int = 1) -> None:
+        """Failure-detection hook: the next persistent launch waits for absent CTAs."""
+        A.check(A.lib().axon_inject_missing_arrival(self._h, missing))
+
     # -- buffers
     def words(self, name: str) -> int:
         return int(A.lib().axon_buf_words(self._h, A.BUF[name]))

@@ -275,6 +275,8 @@ typedef struct axon_serve_counters {
   uint64_t max_batch;  /* most trajectories advanced in one tick */
   double mean_batch;   /* trajectories per tick, mean */
   double busy_s;       /* time spent in ticks */
+  double drive_s;      /* device time of the drive kernel, summed over ticks */
+  double emit_s;       /* device time of the threshold/emit kernel, summed over ticks */
 } axon_serve_counters;
 
 double axon_clock_s(void);
@@ -295,6 +297,13 @@ axon_status axon_serve_destroy(axon_server* s);
 
 /* Grid-wait limit of the persistent kernels in nanoseconds (default 2e9). */
 axon_status axon_set_wait_limit(axon_net* net, uint64_t ns);
+/* No counterpart in the reference (it has no failure detection). Test hook for the bounded
+ * waits: the next persistent launch of this network (axon_present, or axon_multi_train
+ * when the network is nets[0]) waits at every grid barrier for `missing` CTAs that were
+ * never launched, as if they had died. The first barrier then runs out after the wait
+ * limit, every CTA returns, and the call reports AXON_ETIMEOUT; the GPU context stays
+ * usable. One-shot. */
+axon_status axon_inject_missing_arrival(axon_net* net, uint32_t missing);
 /* Text of the last error on this thread. */
 const char* axon_last_error(void);
 
