@@ -92,16 +92,16 @@ def printed(r: dict) -> dict:
             "drive": f"{r['drive_t6']:.0f}"}
 
 
-def bench_multi(dev: int) -> dict:
+def bench_multi(dev: int, nnets: int = 25, epochs: int = EPOCHS) -> dict:
     """25 networks of uneven load (seeds 0-4 x loads 12..60, config C, 40 epochs plus the
     readouts of the five measurements): one persistent launch with an autotuned shape,
     against the plain path running the same presentations one launch each."""
     import axon_b200 as ax
 
-    seeds = [s for s in MULTI_SEEDS for _ in MULTI_LOADS]
-    loads = [L for _ in MULTI_SEEDS for L in MULTI_LOADS]
+    seeds = [s for s in MULTI_SEEDS for _ in MULTI_LOADS][:nnets]
+    loads = [L for _ in MULTI_SEEDS for L in MULTI_LOADS][:nnets]
     nets = [ax.Network(config_c(), device=dev) for _ in seeds]
-    kw = dict(epochs=EPOCHS, T=10, clamp_steps=5, stimcols=STIMCOLS, wave_t=35)
+    kw = dict(epochs=epochs, T=10, clamp_steps=5, stimcols=STIMCOLS, wave_t=35)
     try:
         res_p, rep_p = ax.multi_train(nets, seeds, loads, method="plain", **kw)
         res_m, rep_m = ax.multi_train(nets, seeds, loads, method="launch", autotune=True, graph=True, **kw)
@@ -113,14 +113,15 @@ def bench_multi(dev: int) -> dict:
             for r in json.loads((ROOT / "tests" / "golden" / "published.json").read_text())["table1"]}
     rows = {L: printed(res_m[i]) for i, (s, L) in enumerate(zip(seeds, loads)) if s == 0}
     steps = rep_m["steps"]
-    return {"workload": "25 networks (seeds 0-4 x loads 12,24,36,48,60), config C, 40 epochs + readouts",
+    return {"workload": f"{len(nets)} networks (seeds 0-4 x loads 12,24,36,48,60), config C, {epochs} epochs + readouts",
             "networks": len(nets), "network_steps": steps, "learning_steps": rep_m["train_steps"],
             "one_launch_ms": rep_m["gpu_ms"], "plain_ms": rep_p["gpu_ms"],
             "one_launch_steps_per_s": steps / (rep_m["gpu_ms"] / 1e3),
             "plain_steps_per_s": steps / (rep_p["gpu_ms"] / 1e3), "speedup_vs_plain": rep_p["gpu_ms"] / rep_m["gpu_ms"],
             "shape": {k: rep_m[k] for k in ("slots", "threads", "tiles", "grid", "graph", "tried")},
             "tune_ms": rep_m["tune_ms"], "bit_exact_vs_plain": True,
-            "seed0_rows": rows, "seed0_rows_equal_published_table1": all(rows[L] == gold[L] for L in rows)}
+            "seed0_rows": rows,
+            "seed0_rows_equal_published_table1": epochs == EPOCHS and all(rows[L] == gold[L] for L in rows)}
 
 
 SERVE_LOADS = (12, 36, 60, 100, 140, 170, 200, 200)
@@ -128,33 +129,34 @@ SERVE_RATES = (2000, 10000, 50000)
 SERVE_SECONDS = 1.0
 
 
-def bench_serve(dev: int) -> dict:
+def bench_serve(dev: int, rates=SERVE_RATES, seconds: float = SERVE_SECONDS, nnets: int = len(SERVE_LOADS)) -> dict:
     """Recall serving: 8 trained networks (config C, loads 12..200, seeds 0-7) answer
     Poisson-arriving recall requests (cue = 16-64 of a stored pattern's columns, 5 clamped
     + 10-60 free steps) with continuous batching; latency = result on the host - arrival."""
     import axon_b200 as ax
 
-    seeds = list(range(len(SERVE_LOADS)))
+    loads = list(SERVE_LOADS[:nnets])
+    seeds = list(range(len(loads)))
     nets = [ax.Network(config_c(), device=dev) for _ in seeds]
     try:
-        _, rep = ax.multi_train(nets, seeds, list(SERVE_LOADS), epochs=EPOCHS, T=10, clamp_steps=5, stimcols=STIMCOLS,
+        _, rep = ax.multi_train(nets, seeds, loads, epochs=EPOCHS, T=10, clamp_steps=5, stimcols=STIMCOLS,
                                 readout=False, autotune=True)
-        pats = [ax.stimuli(sd, L, INCOLS, STIMCOLS) for sd, L in zip(seeds, SERVE_LOADS)]
+        pats = [ax.stimuli(sd, L, INCOLS, STIMCOLS) for sd, L in zip(seeds, loads)]
         refs = []  # clamped reference assemblies (active recurrent columns per pattern)
         for net, P in zip(nets, pats):
             cues = np.stack([ax.load_stim(P[q], 1.0, 2000 + q, NCOL) for q in range(len(P))])
             fin = net.recall(cues, 10, 10)["final"]
             refs.append([set(np.nonzero(fin[q, INCOLS:])[0].tolist()) for q in range(len(P))])
-        out = {"workload": "8 networks (config C, loads 12,36,60,100,140,170,200,200, seeds 0-7); Poisson arrivals; "
-                           "cue 16-64 columns of a stored pattern; 5 clamped + 10-60 free steps",
+        out = {"workload": f"{len(nets)} networks (config C, loads {','.join(map(str, loads))}, seeds 0-{len(nets) - 1}); "
+                           "Poisson arrivals; cue 16-64 columns of a stored pattern; 5 clamped + 10-60 free steps",
                "train_ms": rep["gpu_ms"], "rates": []}
         srv = ax.Server(nets, 256 << 20)
         try:
             out["slots"] = srv.stats()["slots"]
             rng = np.random.default_rng(12345)
             tag = 0
-            for rate in SERVE_RATES:
-                n = int(rate * SERVE_SECONDS)
+            for rate in rates:
+                n = int(rate * seconds)
                 gaps = rng.exponential(1.0 / rate, n)
                 reqs = []
                 for i in range(n):
@@ -202,6 +204,18 @@ def bench_serve(dev: int) -> dict:
         for x in nets:
             x.close()
     return out
+
+
+def plain_alg_bytes(hist: np.ndarray, conn: np.ndarray) -> float:
+    """Algorithmic HBM bytes of the plain path over the recorded trajectories: per
+    trajectory-step 1 KiB per (column, branch) whose presynaptic group spiked at t-1
+    (the W3 tiles k_drive must read), plus conn (512 KiB) and the spike vector (16 KiB)."""
+    ngrp = NCOL // 8
+    fan = np.bincount(conn.astype(np.int64), minlength=ngrp).astype(np.float64)
+    act = (hist.reshape(hist.shape[0], hist.shape[1], ngrp, 8) != 0).any(-1)  # group spiked at t
+    tiles = np.zeros(hist.shape[:2])
+    tiles[:, 1:] = (act[:, :-1] * fan).sum(-1)
+    return float((1024.0 * tiles + 512 * 1024 + 16 * 1024).sum())
 
 
 def train(net, pats) -> float:
@@ -372,6 +386,11 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
     ap.add_argument("--no-multi", action="store_true", help="skip the 25-network one-launch measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the recall-serving measurement")
+    ap.add_argument("--multi-nets", type=int, default=25, help="networks of the multi-network block (small cases)")
+    ap.add_argument("--multi-epochs", type=int, default=EPOCHS)
+    ap.add_argument("--serve-rates", default=",".join(map(str, SERVE_RATES)), help="offered loads, requests/s")
+    ap.add_argument("--serve-seconds", type=float, default=SERVE_SECONDS)
+    ap.add_argument("--serve-nets", type=int, default=len(SERVE_LOADS))
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -443,10 +462,17 @@ def main() -> None:
         pt = [net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_final.data_ptr(), method="plain")
               for _ in range(2)]
         pms = max_over_ranks(float(np.mean(pt)), dist)
-        plain = {"value": world * events / (pms / 1e3), "ms_per_step": pms, "launches_per_step": B}
+        hbm_peak, pk = peaks()
+        pa = plain_alg_bytes(ref["hist"], conn) / (pms / 1e3) / 1e9
+        plain = {"value": world * events / (pms / 1e3), "ms_per_step": pms, "launches_per_step": B,
+                 "us_per_trajectory_step": 1e3 * pms / (B * T_RECALL),
+                 "roofline": {"bound": "hbm", "achieved": pa, "peak": hbm_peak, "unit": "GB/s", "frac": pa / hbm_peak,
+                              "peak_kind": pk, "note": "algorithmic bytes = sum over trajectory-steps of 1 KiB per "
+                                                       "(column, branch) with a spiking group + conn + spikes"}}
 
-    multi = None if args.no_multi else bench_multi(dev)
-    serving = None if args.no_serve else bench_serve(dev)
+    multi = None if args.no_multi else bench_multi(dev, args.multi_nets, args.multi_epochs)
+    serving = None if args.no_serve else bench_serve(dev, [int(x) for x in args.serve_rates.split(",")],
+                                                     args.serve_seconds, args.serve_nets)
 
     if rank != 0:
         if dist is not None:
