@@ -78,7 +78,8 @@ class ServeResult(C.Structure):
 class ServeCounters(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("in_flight", C.c_uint32), ("queued", C.c_uint64), ("ticks", C.c_uint64),
                 ("completed", C.c_uint64), ("max_batch", C.c_uint64), ("mean_batch", C.c_double),
-                ("busy_s", C.c_double), ("drive_s", C.c_double), ("emit_s", C.c_double)]
+                ("busy_s", C.c_double), ("drive_s", C.c_double), ("emit_s", C.c_double), ("slot_bytes", C.c_uint64),
+                ("fixed_bytes", C.c_uint64)]
 
 
 class AxonError(RuntimeError):

@@ -8,15 +8,14 @@
 // k_serve_drive: a warp takes one (group of up to 8 trajectories of one network, column)
 // item. It loads each W3 tile that any member needs once and applies it to every member
 // whose presynaptic group is active, so the weights are read once per column per group
-// instead of once per trajectory; per member it forms the exact k-of-32 ballot and the
-// column drive.
-// k_serve_emit: a CTA per trajectory selects the column threshold over its drive vector
-// and rebuilds its spike vector and group-activity bits; a trajectory on its last step
-// also copies its final spikes to the done buffer.
+// instead of once per trajectory; it writes each member's per-neuron drives and column drive.
+// k_serve_emit: a CTA per trajectory selects the column threshold over its drive vector,
+// runs the exact k-of-32 only for the columns that pass the gate (the others cannot spike),
+// and writes the spike vector and group-activity bits; a trajectory on its last step also
+// copies its final spikes to the done buffer.
 #include <cstdint>
 
 #include "axon_device.cuh"
-#include "emit.cuh"
 #include "serve.cuh"
 #include "theta.cuh"
 
@@ -94,13 +93,10 @@ __global__ void __launch_bounds__(kServeThreads, 3) k_serve_drive(ServeDev d, Se
       uint32_t a = acc[j];
       if (c.facil != 0u && spkIn[j] && ((__ldg(spkIn[j] + cc) >> lane) & 1u)) a += c.facil;
       const uint32_t drv = __reduce_add_sync(kFull, a);
-      uint32_t vk, vk1;
-      const uint32_t ball = warp_kwta(a, lane, c.k, vk, vk1);
-      if (lane == 0) {
-        uint32_t* base = d.slots + (size_t)d.ent[G.e[j]].slot * d.slotWords + 2u * ncol + 2u * d.nactw;
-        __stcg(base + cc, drv);          // xdrive
-        __stcg(base + ncol + cc, ball);  // xball
-      }
+      uint32_t* base = d.slots + (size_t)d.ent[G.e[j]].slot * d.slotWords;
+      if (c.acc32) __stcg(base + serve_acc_off(ncol) + cc * 32u + lane, a);
+      else __stcg(reinterpret_cast<unsigned short*>(base + serve_acc_off(ncol)) + cc * 32u + lane, (unsigned short)a);
+      if (lane == 0) __stcg(base + 2u * ncol + 2u * d.nactw + cc, drv);  // xdrive
     }
   }
 }
@@ -109,19 +105,23 @@ __global__ void __launch_bounds__(kServeThreads) k_serve_emit(ServeDev d, ServeC
   extern __shared__ __align__(16) uint32_t sm[];
   const uint32_t ncol = c.ncol, incols = c.incols, ngrp = ncol / 8u;
   uint32_t* sD = sm;
-  uint32_t* sStim = sD + ncol;
+  uint32_t* sSpk = sD + ncol;
+  uint32_t* sList = sSpk + ncol;
+  uint32_t* sStim = sList + ncol;
   uint32_t* sHist = sStim + ((incols + 3u) & ~3u);
   uint32_t* sRed = sHist + 256;
-  const uint32_t tid = threadIdx.x, nent = d.counts[0];
+  uint32_t* sCnt = sRed + 192;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
+  const uint32_t nent = d.counts[0];
   for (uint32_t ei = blockIdx.x; ei < nent; ei += gridDim.x) {
     const ServeEntry e = d.ent[ei];
     uint32_t* base = d.slots + (size_t)e.slot * d.slotWords;
     const uint32_t* xdrive = base + 2u * ncol + 2u * d.nactw;
-    const uint32_t* xball = xdrive + ncol;
     for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x)
       cp_async16(reinterpret_cast<uint4*>(sD) + i, reinterpret_cast<const uint4*>(xdrive) + i);
     cp_async_commit();
     const bool clamp = e.tloc < e.clamp;
+    if (tid == 0) sCnt[0] = 0u;
     if (clamp) {  // clamp words of the cue (src/axon.mm:800-804: 0xFFFFFFFF on the cue's columns)
       for (uint32_t i = tid; i < incols; i += blockDim.x) sStim[i] = 0u;
       __syncthreads();
@@ -133,20 +133,51 @@ __global__ void __launch_bounds__(kServeThreads) k_serve_emit(ServeDev d, ServeC
     cp_async_wait<0>();
     __syncthreads();
     const uint32_t theta = block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed, 0u);
+    const uint32_t gate = max(theta, 1u);
+    // k_emit's gate and clamp (src/axon.mm:211-212): clamped input columns take the cue,
+    // other columns spike only when their drive reaches the gate
+    for (uint32_t cc = tid; cc < ncol; cc += blockDim.x) {
+      uint32_t v = 0u;
+      if (clamp && cc < incols) v = sStim[cc];
+      else if (sD[cc] >= gate) sList[atomicAdd(sCnt, 1u)] = cc;
+      sSpk[cc] = v;
+    }
+    __syncthreads();
+    const uint32_t npend = sCnt[0];
+    const uint32_t* accW = base + serve_acc_off(ncol);
+    for (uint32_t p = warp; p < npend; p += nw) {  // exact k-of-32 of the gated columns
+      const uint32_t cc = sList[p];
+      const uint32_t a = c.acc32 ? __ldcg(accW + cc * 32u + lane)
+                                 : (uint32_t)__ldcg(reinterpret_cast<const unsigned short*>(accW) + cc * 32u + lane);
+      uint32_t vk, vk1;
+      const uint32_t ball = warp_kwta(a, lane, c.k, vk, vk1);
+      if (lane == 0) sSpk[cc] = ball;
+    }
+    __syncthreads();
     uint32_t* spkOut = base + (e.tloc & 1u) * ncol;
     uint32_t* actOut = base + 2u * ncol + (e.tloc & 1u) * d.nactw;
-    emit_groups(sD, xball, sStim, spkOut, actOut, max(theta, 1u), clamp, incols, ngrp);
-    if (e.done != 0xFFFFFFFFu) {
-      __syncthreads();
-      uint4* dst = reinterpret_cast<uint4*>(d.doneBuf + (size_t)e.done * ncol);
-      for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x) dst[i] = __ldcg(reinterpret_cast<const uint4*>(spkOut) + i);
+    uint4* dst = e.done != 0xFFFFFFFFu ? reinterpret_cast<uint4*>(d.doneBuf + (size_t)e.done * ncol) : nullptr;
+    for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x) {
+      const uint4 v = reinterpret_cast<const uint4*>(sSpk)[i];
+      __stcg(reinterpret_cast<uint4*>(spkOut) + i, v);
+      if (dst) dst[i] = v;
+    }
+    for (uint32_t gb = warp * 32u; gb < ngrp; gb += nw * 32u) {  // group-activity bits
+      const uint32_t g = gb + lane;
+      bool any = false;
+      if (g < ngrp) {
+        const uint4 p = reinterpret_cast<const uint4*>(sSpk)[2 * g], q = reinterpret_cast<const uint4*>(sSpk)[2 * g + 1];
+        any = (p.x | p.y | p.z | p.w | q.x | q.y | q.z | q.w) != 0u;
+      }
+      const uint32_t wv = __ballot_sync(kFull, any);
+      if (lane == 0) __stcg(actOut + (gb >> 5), wv);
     }
     __syncthreads();
   }
 }
 
 size_t serve_emit_smem_bytes(uint32_t ncol, uint32_t incols) {
-  return ((size_t)ncol + ((incols + 3u) & ~3u) + 256 + 192) * 4;
+  return (3ull * ncol + ((incols + 3u) & ~3u) + 256 + 192 + 4) * 4;
 }
 
 cudaError_t serve_prepare(size_t emitSmem) {

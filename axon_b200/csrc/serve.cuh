@@ -38,7 +38,7 @@ struct ServeGroup {
 
 struct ServeDev {
   const ServeNet* nets;
-  uint32_t* slots;           // slot s at slots + s * slotWords: spk[2][ncol], act[2][nactw], xdrive[ncol], xball[ncol]
+  uint32_t* slots;           // slot s at slots + s * slotWords: spk[2][ncol], act[2][nactw], xdrive[ncol], acc[ncol*32]
   const ServeEntry* ent;
   const ServeGroup* grp;
   const uint32_t* counts;    // [0] entries, [1] groups
@@ -48,15 +48,16 @@ struct ServeDev {
 };
 
 struct ServeCfg {
-  uint32_t ncol, incols, dthr, boost, mode, targetCols, k, facil, topkPar, pad;
+  uint32_t ncol, incols, dthr, boost, mode, targetCols, k, facil, topkPar;
+  uint32_t acc32;  // per-neuron drive kept as u32 (u16 would overflow), else u16
 };
 
-// words of one slot's buffers
-inline uint32_t serve_slot_words(uint32_t ncol) {
-  const uint32_t nactw = ((((ncol / 8u) + 31u) / 32u) + 3u) & ~3u;
-  return (4u * ncol + 2u * nactw + 63u) & ~63u;  // 256-byte multiple
+__host__ __device__ inline uint32_t serve_nactw(uint32_t ncol) { return ((((ncol / 8u) + 31u) / 32u) + 3u) & ~3u; }
+// offset (words) of the per-neuron drives in a slot, and the slot's size (256-byte multiple)
+__host__ __device__ inline uint32_t serve_acc_off(uint32_t ncol) { return (3u * ncol + 2u * serve_nactw(ncol) + 63u) & ~63u; }
+__host__ __device__ inline uint32_t serve_slot_words(uint32_t ncol, uint32_t acc32) {
+  return (serve_acc_off(ncol) + (acc32 ? 32u : 16u) * ncol + 63u) & ~63u;
 }
-inline uint32_t serve_nactw(uint32_t ncol) { return ((((ncol / 8u) + 31u) / 32u) + 3u) & ~3u; }
 
 size_t serve_emit_smem_bytes(uint32_t ncol, uint32_t incols);
 cudaError_t serve_prepare(size_t emitSmem);

@@ -54,6 +54,7 @@ struct axon_server {
   std::vector<axon_net*> nets;
   int device = 0, sms = 0;
   uint32_t ncol = 0, incols = 0, nslots = 0;
+  uint64_t slotCost = 0, fixedCost = 0;  // device bytes per trajectory slot, and fixed
   ServeCfg cfg{};
   size_t emitSmem = 0;
   cudaStream_t stream = nullptr;
@@ -115,13 +116,18 @@ axon_status axon_server::start(axon_net* const* ns, uint32_t n, uint64_t memByte
   const PresentCfg pc = n0->present_cfg(1, 0, false, 0);  // readout parameters (learn = 0)
   cfg.ncol = ncol; cfg.incols = incols; cfg.dthr = pc.dthr; cfg.boost = pc.boost; cfg.mode = pc.mode;
   cfg.targetCols = pc.targetCols; cfg.k = pc.k; cfg.facil = pc.facil; cfg.topkPar = pc.topkPar;
+  // per-neuron drive fits 16 bits unless one neuron's branches can add up past 65535
+  const uint64_t maxAcc = (cfg.mode == 2 ? 32ull : 32ull * (256ull + cfg.boost)) + cfg.facil;
+  cfg.acc32 = maxAcc > 65535ull ? 1u : 0u;
   CKS(cudaSetDevice(device));
   // one slot: its buffers, its share of the done buffer and of the tick tables
-  const size_t slotBytes = (size_t)serve_slot_words(ncol) * 4;
+  const size_t slotBytes = (size_t)serve_slot_words(ncol, cfg.acc32) * 4;
   const size_t perSlot = slotBytes + (size_t)ncol * 4 + sizeof(ServeEntry) + sizeof(ServeGroup) + (size_t)incols * 4;
   const uint64_t fixed = al(n * sizeof(ServeNet)) + 4 * 256 + al(n * sizeof(ServeGroup));
   if (memBytes <= fixed + perSlot) return set_error(AXON_EINVAL, "memory budget below one trajectory slot");
   nslots = (uint32_t)std::min<uint64_t>((memBytes - fixed) / (perSlot + 64), 1u << 16);
+  slotCost = perSlot + 64;
+  fixedCost = fixed;
   stageBytes = 256 + al(nslots * sizeof(ServeEntry)) + al((nslots + n) * sizeof(ServeGroup)) +
                al((size_t)nslots * incols * 4);
   const size_t netsOff = 0, slotsOff = al(n * sizeof(ServeNet)), stageOff = slotsOff + al((size_t)nslots * slotBytes),
@@ -143,7 +149,7 @@ axon_status axon_server::start(axon_net* const* ns, uint32_t n, uint64_t memByte
   dev.slots = (uint32_t*)(b + slotsOff);
   dev.counts = (const uint32_t*)(b + stageOff);  // entries, groups and cues follow, packed per tick
   dev.doneBuf = (uint32_t*)(b + doneOff);
-  dev.slotWords = serve_slot_words(ncol);
+  dev.slotWords = serve_slot_words(ncol, cfg.acc32);
   dev.nactw = serve_nactw(ncol);
   emitSmem = serve_emit_smem_bytes(ncol, incols);
   CKS(serve_prepare(emitSmem));
@@ -385,6 +391,8 @@ axon_status axon_serve_stats(axon_server* s, axon_serve_counters* out) {
   std::lock_guard<std::mutex> g(s->mu);
   std::memset(out, 0, sizeof(*out));
   out->slots = s->nslots;
+  out->slot_bytes = s->slotCost;
+  out->fixed_bytes = s->fixedCost;
   out->ticks = s->ticks;
   out->completed = s->completed;
   out->mean_batch = s->ticks ? (double)s->sumActive / s->ticks : 0.0;

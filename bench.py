@@ -150,7 +150,7 @@ def bench_serve(dev: int, rates=SERVE_RATES, seconds: float = SERVE_SECONDS, nne
         out = {"workload": f"{len(nets)} networks (config C, loads {','.join(map(str, loads))}, seeds 0-{len(nets) - 1}); "
                            "Poisson arrivals; cue 16-64 columns of a stored pattern; 5 clamped + 10-60 free steps",
                "train_ms": rep["gpu_ms"], "rates": []}
-        srv = ax.Server(nets, 256 << 20)
+        srv = ax.Server(nets, 1 << 30)
         try:
             out["slots"] = srv.stats()["slots"]
             rng = np.random.default_rng(12345)

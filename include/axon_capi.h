@@ -277,6 +277,8 @@ typedef struct axon_serve_counters {
   double busy_s;       /* time spent in ticks */
   double drive_s;      /* device time of the drive kernel, summed over ticks */
   double emit_s;       /* device time of the threshold/emit kernel, summed over ticks */
+  uint64_t slot_bytes; /* device memory one trajectory slot takes */
+  uint64_t fixed_bytes;/* device memory of the server besides its slots: slots = (mem_bytes - fixed) / slot */
 } axon_serve_counters;
 
 double axon_clock_s(void);

@@ -81,9 +81,10 @@ def test_staggered_arrivals_and_few_slots(fleet):
     reqs = requests(pats, 40, 2)
     base, _ = serve(nets, reqs)
     staggered, _ = serve(nets, reqs, spread_s=0.05)
-    slot_bytes = 4 * (4 * 512 + 8) + 4 * 512 + 32 + 40 + 4 * 64 + 64
-    few, st = serve(nets, reqs, mem_bytes=3 * slot_bytes + 8192)
-    assert st["slots"] <= 4 and st["max_batch"] <= st["slots"]
+    with ax.Server(nets, 16 << 20) as probe:
+        cost = probe.stats()
+    few, st = serve(nets, reqs, mem_bytes=cost["fixed_bytes"] + 3 * cost["slot_bytes"] + 100)
+    assert st["slots"] == 3 and st["max_batch"] <= 3  # admission is bounded by the memory budget
     for r in reqs:
         t = r["tag"]
         assert np.array_equal(base[t][1], staggered[t][1]) and np.array_equal(base[t][1], few[t][1]), t
