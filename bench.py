@@ -277,35 +277,6 @@ def peaks() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def dist_setup(gpus: int):
-    if gpus <= 1 or "RANK" not in os.environ:
-        return 0, 1, None
-    import torch
-    import torch.distributed as dist
-
-    rank, world = int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
-    from datetime import timedelta
-
-    dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    return rank, world, dist
-
-
-def barrier(dist):
-    if dist is not None:
-        dist.barrier()
-
-
-def max_over_ranks(x: float, dist) -> float:
-    if dist is None:
-        return x
-    import torch
-
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
 def cpu_sample(cfg, gpu_net, cues, ev, threads: int, ntraj: int) -> dict:
     """The CPU oracle on a bounded sample of the same trajectories (same trained state)."""
     sys.path.insert(0, str(ROOT / "tests"))
@@ -396,7 +367,10 @@ def main() -> None:
         run_reference(args)
         return
     assert args.warmup >= 3, "at least 3 warm-up steps"
-    rank, world, dist = dist_setup(args.gpus)
+    from axon_b200.replicas import Replicas
+
+    rep = Replicas.from_env(args.gpus)
+    rank, world = rep.rank, rep.world
     import torch
 
     import axon_b200 as ax
@@ -404,7 +378,7 @@ def main() -> None:
 
     if rank == 0:
         build.build_lib()
-    barrier(dist)
+    rep.barrier()
     dev = torch.cuda.current_device()
     cfg = config_c()
     net = ax.Network(cfg, device=dev)
@@ -429,15 +403,15 @@ def main() -> None:
     assert np.array_equal(d_final.cpu().numpy().view(np.uint32), ref["final"])
     times = []
     torch.cuda.synchronize()
-    barrier(dist)
+    rep.barrier()
     with ClockSampler(dev) as clk:
         for _ in range(args.steps):
             flush.zero_()  # evict L2 between timed steps (untimed: outside the device-timed launch)
             torch.cuda.synchronize()
             times.append(net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_final.data_ptr()))
         torch.cuda.synchronize()
-    barrier(dist)
-    ms = max_over_ranks(float(np.mean(times)), dist)
+    rep.barrier()
+    ms = rep.max(float(np.mean(times)))
     value = world * events / (ms / 1e3)
 
     # end to end through the public C-ABI call with pinned host buffers
@@ -452,7 +426,7 @@ def main() -> None:
             e2e_t.append(dt)
     if e2e_t:
         assert np.array_equal(r["final"], ref["final"])
-    e2e_s = max_over_ranks(float(np.mean(e2e_t)) if e2e_t else float("nan"), dist)
+    e2e_s = rep.max(float(np.mean(e2e_t)) if e2e_t else float("nan"))
 
     # plain GPU path on the same 300 trajectories (one persistent launch per trajectory)
     plain = None
@@ -461,7 +435,7 @@ def main() -> None:
         assert np.array_equal(rp["final"], ref["final"])
         pt = [net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_final.data_ptr(), method="plain")
               for _ in range(2)]
-        pms = max_over_ranks(float(np.mean(pt)), dist)
+        pms = rep.max(float(np.mean(pt)))
         hbm_peak, pk = peaks()
         pa = plain_alg_bytes(ref["hist"], conn) / (pms / 1e3) / 1e9
         plain = {"value": world * events / (pms / 1e3), "ms_per_step": pms, "launches_per_step": B,
@@ -475,8 +449,7 @@ def main() -> None:
                                                      args.serve_seconds, args.serve_nets)
 
     if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
+        rep.close()
         return
     hbm, peak_kind = peaks()
     # roofline of the batched kernel: W3 (128 MiB, read once per recall step for all
@@ -511,8 +484,7 @@ def main() -> None:
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    rep.close()
 
 
 if __name__ == "__main__":
