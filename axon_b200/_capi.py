@@ -70,6 +70,11 @@ class MultiReport(C.Structure):
 MULTI_ONE_LAUNCH, MULTI_PLAIN = 0, 1
 
 
+class CkptMeta(C.Structure):
+    _fields_ = [("seed", C.c_uint32), ("nstim", C.c_uint32), ("stimcols", C.c_uint32), ("epochs", C.c_uint32),
+                ("reserved", C.c_uint32 * 4)]
+
+
 class ServeResult(C.Structure):
     _fields_ = [("tag", C.c_uint64), ("net", C.c_uint32), ("steps", C.c_uint32), ("arrive_s", C.c_double),
                 ("admit_s", C.c_double), ("done_s", C.c_double)]
@@ -124,6 +129,8 @@ def lib() -> C.CDLL:
                                           C.c_uint32]
         L.axon_multi_train.argtypes = [C.POINTER(C.c_void_p), C.c_uint32, U32P, U32P, C.POINTER(MultiArgs),
                                        C.POINTER(MultiResult), C.POINTER(MultiReport)]
+        L.axon_save.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(CkptMeta)]
+        L.axon_load.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(CkptMeta)]
         L.axon_clock_s.restype = C.c_double
         L.axon_serve_create.argtypes = [C.POINTER(C.c_void_p), C.c_uint32, C.c_uint64, C.POINTER(C.c_void_p)]
         L.axon_serve_submit.argtypes = [C.c_void_p, C.c_uint32, U32P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,

@@ -72,6 +72,18 @@ class Network:
         """Failure-detection hook: the next persistent launch waits for absent CTAs."""
         A.check(A.lib().axon_inject_missing_arrival(self._h, missing))
 
+    # -- checkpoints
+    def save(self, path: str, seed: int, nstim: int, stimcols: int, epochs: int) -> None:
+        """Writes the trained state (W0..W3, conn, bias, mult) and its metadata to `path`."""
+        m = A.CkptMeta(seed=seed, nstim=nstim, stimcols=stimcols, epochs=epochs)
+        A.check(A.lib().axon_save(self._h, str(path).encode(), C.byref(m)))
+
+    def load(self, path: str) -> dict:
+        """Replaces the state with a checkpoint's (same configuration required); returns its metadata."""
+        m = A.CkptMeta()
+        A.check(A.lib().axon_load(self._h, str(path).encode(), C.byref(m)))
+        return {"seed": m.seed, "nstim": m.nstim, "stimcols": m.stimcols, "epochs": m.epochs}
+
     # -- buffers
     def words(self, name: str) -> int:
         return int(A.lib().axon_buf_words(self._h, A.BUF[name]))

@@ -188,6 +188,25 @@ typedef struct axon_state_dev {
 axon_status axon_present_static(const axon_cfg* cfg, const axon_state_dev* state, uint32_t T,
                                 uint32_t clamp_steps, int learn, uint32_t use_bias);
 
+/* ---------------------------------------------------------------- checkpoints
+ * The reference keeps no trained network: each run retrains from the seed
+ * (src/axon.mm:1001-1033). A checkpoint file holds one network's trained state - the
+ * W0..W3 planes, conn, bias and mult (the MTLBuffers of src/axon.mm:749-768) - with its
+ * axon_cfg and the caller's training metadata, each section and the whole file under an
+ * FNV-1a-64 checksum. axon_load verifies magic, version, configuration (it must equal the
+ * network's) and checksums before it changes the network; on success the network is
+ * initialised, its stats and theta cleared. */
+typedef struct axon_ckpt_meta {
+  uint32_t seed;        /* [seed] the network and its patterns were made from */
+  uint32_t nstim;       /* [stim] patterns stored (the load) */
+  uint32_t stimcols;    /* [stimcols] columns per pattern */
+  uint32_t epochs;      /* [epochs] trained */
+  uint32_t reserved[4]; /* zero */
+} axon_ckpt_meta;
+
+axon_status axon_save(axon_net* net, const char* path, const axon_ckpt_meta* meta);
+axon_status axon_load(axon_net* net, const char* path, axon_ckpt_meta* meta_out);
+
 /* ---------------------------------------------------------------- many networks, one launch
  * The reference trains and reads out one network per process: build/axon runs init,
  * epochs x nstim learning presentations plus one more of pattern 0 (src/axon.mm:1001-1033),
