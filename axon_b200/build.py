@@ -24,7 +24,7 @@ ORACLE_DIR = ROOT / "oracle"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
-LIB_SOURCES = ["plain.cu", "batch.cu", "multi.cu", "serve.cu", "engine.cu", "recall.cu", "multi_host.cu", "serve_host.cu",
+LIB_SOURCES = ["plain.cu", "batch.cu", "multi.cu", "serve.cu", "serve_batched.cu", "engine.cu", "recall.cu", "multi_host.cu", "serve_host.cu",
                "capi.cu", "static_present.cu", "checkpoint.cu"]
 CLI_SOURCES = ["cli_main.cpp", "protocol.cpp"]
 

@@ -21,14 +21,10 @@
 
 #include "axon_device.cuh"
 #include "batch.cuh"
+#include "batch_common.cuh"
 #include "theta.cuh"
 
 namespace axon {
-
-// Tile layout for the batched kernel: word w of row r of a (column, branch) tile is stored
-// at w*32 + ((r + 4w) mod 32). Rows r..r+3 (r a multiple of 4) of one word are then 16
-// contiguous bytes, and lanes reading different words hit different groups of 4 banks.
-__host__ __device__ __forceinline__ uint32_t w3r_pos(uint32_t r, uint32_t w) { return w * 32u + ((r + 4u * w) & 31u); }
 
 __global__ void k_make_w3r(const uint4* __restrict__ W3, uint32_t* __restrict__ W3R, uint64_t ntile) {
   // one thread per (tile, row): scatters the row's 8 words
@@ -46,66 +42,6 @@ cudaError_t launch_make_w3r(const uint4* W3, uint32_t* W3R, uint32_t ncol, cudaS
   const uint64_t ntile = (uint64_t)ncol * kNslot;
   k_make_w3r<<<(unsigned)((ntile * 32 + 255) / 256), 256, 0, st>>>(W3, W3R, ntile);
   return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------- TMA bulk copy + mbarrier
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-// bounded wait for one phase of an mbarrier
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
-  if (mbar_test(bar, parity)) return true;
-  const uint64_t t0 = globaltimer_ns();
-  for (uint32_t it = 1;; ++it) {
-    if (mbar_test(bar, parity)) return true;
-    if ((it & 255u) == 0u && globaltimer_ns() - t0 > limit_ns) return false;
-  }
-}
-
-// dendritic nonlinearity of k_drive, src/axon.mm:174-178, applied to a non-silent branch.
-// LIN (modes 0, 1): count plus bst when the count reaches dthr; otherwise (mode 2) 0 or 1.
-template <bool LIN>
-__device__ __forceinline__ uint32_t branch_term(uint32_t cnt, uint32_t dthr, uint32_t bst) {
-  if (LIN) return cnt + (cnt >= dthr ? bst : 0u);
-  return cnt >= dthr ? 1u : 0u;
-}
-
-constexpr uint32_t kColWords = kNslot * 256;             // one column's 32 tiles
-constexpr uint64_t kDrainNs = 1000000000ull;             // bound on waiting for own copies after a timeout
-constexpr uint32_t kItemWords = kRecallCpi * kColWords;  // one work item
-
-template <bool PACK>
-__device__ __forceinline__ void acc_add4(uint32_t* accb, uint32_t r, uint32_t t0, uint32_t t1, uint32_t t2,
-                                         uint32_t t3) {
-  if (PACK) {
-    atomicAdd(accb + (r >> 1), t0 | (t1 << 16));
-    atomicAdd(accb + (r >> 1) + 1, t2 | (t3 << 16));
-  } else {
-    atomicAdd(accb + r, t0);
-    atomicAdd(accb + r + 1, t1);
-    atomicAdd(accb + r + 2, t2);
-    atomicAdd(accb + r + 3, t3);
-  }
 }
 
 template <bool PACK, bool LIN>

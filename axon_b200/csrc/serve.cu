@@ -162,6 +162,35 @@ __global__ void __launch_bounds__(kServeThreads) k_serve_emit(ServeDev d, ServeC
       __stcg(reinterpret_cast<uint4*>(spkOut) + i, v);
       if (dst) dst[i] = v;
     }
+    if (e.nextIdx != 0xFFFFFFFFu) {  // entry lists of the next tick: groups with spikes, their nonzero words
+      const ServeNet net = d.nets[e.net];
+      const uint32_t q = d.par ^ 1u;
+      uint2* e1Out = net.ent1 + (size_t)q * ngrp * kServeMaxB;
+      uint4* eMOut = net.entM + (size_t)q * ngrp * kServeMaxB;
+      uint32_t* c1Out = net.ecnt + (size_t)q * 2 * ngrp;
+      uint32_t* cMOut = c1Out + ngrp;
+      for (uint32_t g = tid; g < ngrp; g += blockDim.x) {
+        const uint4 p = reinterpret_cast<const uint4*>(sSpk)[2 * g], q4 = reinterpret_cast<const uint4*>(sSpk)[2 * g + 1];
+        const uint32_t w[8] = {p.x, p.y, p.z, p.w, q4.x, q4.y, q4.z, q4.w};
+        uint32_t nz = 0, S0 = 0u, S1 = 0u, S2 = 0u, k = 0, w0 = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          if (w[i]) {
+            nz |= 1u << i;
+            if (k == 0) { S0 = w[i]; w0 = (uint32_t)i; }
+            else if (k == 1) S1 = w[i];
+            else if (k == 2) S2 = w[i];
+            ++k;
+          }
+        if (k == 1) {
+          const uint32_t at = atomicAdd(c1Out + g, 1u);
+          __stcg(e1Out + (size_t)g * kServeMaxB + at, make_uint2(e.nextIdx | (w0 << 16), S0));
+        } else if (k > 1) {
+          const uint32_t at = atomicAdd(cMOut + g, 1u);
+          __stcg(eMOut + (size_t)g * kServeMaxB + at, make_uint4(e.nextIdx | (nz << 16), S0, S1, S2));
+        }
+      }
+    }
     for (uint32_t gb = warp * 32u; gb < ngrp; gb += nw * 32u) {  // group-activity bits
       const uint32_t g = gb + lane;
       bool any = false;
@@ -184,12 +213,31 @@ cudaError_t serve_prepare(size_t emitSmem) {
   return cudaFuncSetAttribute(k_serve_emit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)emitSmem);
 }
 
-cudaError_t launch_serve_tick(const ServeDev& d, const ServeCfg& c, int sms, size_t emitSmem, cudaStream_t st,
-                              cudaEvent_t between) {
-  k_serve_drive<<<sms * 8, kServeThreads, 0, st>>>(d, c);
-  cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess && between) e = cudaEventRecord(between, st);
-  if (e != cudaSuccess) return e;
+// list lengths of the next tick start at zero (every network, parity par ^ 1)
+__global__ void k_serve_zero_counts(ServeDev d, uint32_t nnets, uint32_t ngrp) {
+  const uint32_t q = d.par ^ 1u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nnets * 2u * ngrp; i += gridDim.x * blockDim.x) {
+    const uint32_t n = i / (2u * ngrp), j = i - n * 2u * ngrp;
+    d.nets[n].ecnt[(size_t)q * 2 * ngrp + j] = 0u;
+  }
+}
+
+cudaError_t launch_serve_batched(const ServeDev& d, const ServeCfg& c, int sms, cudaStream_t st);
+
+cudaError_t launch_serve_drive(const ServeDev& d, const ServeCfg& c, int sms, bool gather, bool batched,
+                               cudaStream_t st) {
+  if (gather) {
+    k_serve_drive<<<sms * 8, kServeThreads, 0, st>>>(d, c);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (batched) return launch_serve_batched(d, c, sms, st);
+  return cudaSuccess;
+}
+
+cudaError_t launch_serve_emit(const ServeDev& d, const ServeCfg& c, int sms, size_t emitSmem, cudaStream_t st,
+                              uint32_t nnets) {
+  k_serve_zero_counts<<<16, 256, 0, st>>>(d, nnets, c.ncol / 8u);
   k_serve_emit<<<sms * 6, kServeThreads, emitSmem, st>>>(d, c);
   return cudaGetLastError();
 }

@@ -1,0 +1,245 @@
+// Batched drive of the recall server: one tick's drive step for every trajectory of the
+// networks that have many trajectories in flight (k_drive, src/axon.mm:150-190, learn = 0).
+//
+// Work items are (network, column pair) claimed dynamically by every CTA. An item's 64
+// W3 tiles (64 KiB, batched layout) arrive by TMA bulk copies into shared memory,
+// double-buffered across items, so each tile is read once per tick for all of the
+// network's trajectories. The per-group entry lists written by the previous tick's emit
+// kernel name, for each presynaptic group, the trajectories whose group spiked and their
+// nonzero spike words; lanes take (branch, entry) pairs and AND-popcount the entry's
+// words against all 32 rows of the tile into per-(trajectory, neuron) counters in shared
+// memory (two 16-bit sums per 32-bit atomic when they fit). The counters become each
+// trajectory's per-neuron drives and column drives in its slot. Trajectories are
+// independent, so this kernel needs no grid barrier: the emit kernel that follows in the
+// stream finishes the step.
+#include <cstdint>
+
+#include "axon_device.cuh"
+#include "batch_common.cuh"
+#include "serve.cuh"
+
+namespace axon {
+
+namespace {
+template <bool PACK>
+__host__ __device__ constexpr uint32_t sb_stride() { return PACK ? 17u : 33u; }
+template <bool PACK>
+__host__ __device__ constexpr uint32_t sb_maxb() { return PACK ? kServeMaxB : kServeMaxB32; }
+}  // namespace
+
+template <bool PACK, bool LIN>
+__global__ void __launch_bounds__(1024, 1) k_serve_batched(ServeDev d, ServeCfg c) {
+  extern __shared__ __align__(128) uint32_t sm[];
+  const uint32_t ncol = c.ncol, ngrp = ncol / 8u, dthr = c.dthr, bst = c.bst;
+  constexpr uint32_t accStride = sb_stride<PACK>();
+  constexpr uint32_t maxB = sb_maxb<PACK>();
+  uint32_t* sTile = sm;                                     // [2][kItemWords]
+  uint32_t* sAcc = sTile + 2 * kItemWords;                  // [kRecallCpi][B][accStride]
+  uint32_t* sConn = sAcc + kRecallCpi * maxB * accStride;   // [64]
+  uint32_t* sP1 = sConn + 64;                               // [68] single-word entries: prefix over 64 branches
+  uint32_t* sPM = sP1 + 68;                                 // [68] multi-word entries
+  uint32_t* sMisc = sPM + 68;                               // [16]
+  uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
+  const uint32_t nip = (ncol + kRecallCpi - 1) / kRecallCpi;  // work items per network
+  const uint32_t nitems = d.counts[3];
+  if (nitems == 0u) return;
+  if (tid == 0) {
+    mbar_init(&sBar[0], 1);
+    mbar_init(&sBar[1], 1);
+    fence_proxy_async_smem();
+  }
+  __syncthreads();
+  uint32_t uses0 = 0, uses1 = 0, kbuf = 0;
+
+  auto issue = [&](uint32_t it, uint32_t buf) {  // thread 0 only
+    const uint32_t* W3R = d.nets[d.bnets[it / nip].net].W3R;
+    const uint32_t c0 = (it % nip) * kRecallCpi;
+    const uint32_t ncols = min(kRecallCpi, ncol - c0);
+    fence_proxy_async_smem();
+    mbar_expect_tx(&sBar[buf], ncols * kColWords * 4u);
+    for (uint32_t k = 0; k < ncols; ++k)
+      bulk_g2s(sTile + buf * kItemWords + k * kColWords, W3R + (size_t)(c0 + k) * kColWords, kColWords * 4u, &sBar[buf]);
+  };
+  auto spk_prev = [&](uint32_t tabOff, uint32_t b) -> const uint32_t* {  // spk(t-1) of batch index b
+    const uint2 st = __ldg(d.btab + tabOff + b);
+    return d.slots + (size_t)st.x * d.slotWords + ((st.y - 1u) & 1u) * ncol;
+  };
+
+  if (tid == 0) {
+    const uint32_t it0 = atomicAdd(d.work, 1u);
+    sMisc[1] = it0;
+    if (it0 < nitems) issue(it0, kbuf);
+  }
+  __syncthreads();
+  uint32_t item = sMisc[1];
+  while (item < nitems) {
+    const uint32_t bcur = kbuf;
+    if (tid == 0) {
+      const uint32_t nx = atomicAdd(d.work, 1u);
+      sMisc[2] = nx;
+      sMisc[3] = 0u;
+      if (nx < nitems) issue(nx, bcur ^ 1u);
+    }
+    const ServeBNet bn = d.bnets[item / nip];
+    const uint32_t* conn = d.nets[bn.net].conn;
+    const uint2* e1In = d.nets[bn.net].ent1 + (size_t)d.par * ngrp * kServeMaxB;
+    const uint4* eMIn = d.nets[bn.net].entM + (size_t)d.par * ngrp * kServeMaxB;
+    const uint32_t* c1In = d.nets[bn.net].ecnt + (size_t)d.par * 2 * ngrp;
+    const uint32_t* cMIn = c1In + ngrp;
+    const uint32_t B = bn.B;
+    const uint32_t c0 = (item % nip) * kRecallCpi;
+    for (uint32_t i = tid; i < 64u; i += blockDim.x) {
+      const uint32_t col = c0 + (i >> 5);
+      sConn[i] = col < ncol ? __ldg(conn + col * kNslot + (i & 31u)) : 0u;
+    }
+    for (uint32_t i = tid; i < kRecallCpi * B * accStride; i += blockDim.x) sAcc[i] = 0u;
+    __syncthreads();
+    if (warp < 2) {  // prefixes of the 64 list lengths, single-word (warp 0) and multi-word (warp 1)
+      const uint32_t* cin = warp ? cMIn : c1In;
+      uint32_t* P = warp ? sPM : sP1;
+      const bool v1 = c0 + 1 < ncol;
+      const uint32_t n0 = __ldcg(cin + sConn[lane]), n1 = v1 ? __ldcg(cin + sConn[32 + lane]) : 0u;
+      uint32_t i0 = n0, i1 = n1;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t a = __shfl_up_sync(kFull, i0, off), b = __shfl_up_sync(kFull, i1, off);
+        if (lane >= (uint32_t)off) { i0 += a; i1 += b; }
+      }
+      const uint32_t tot0 = __shfl_sync(kFull, i0, 31);
+      P[1 + lane] = i0;
+      P[33 + lane] = tot0 + i1;
+      if (lane == 0) P[0] = 0u;
+    }
+    const uint32_t parCur = (bcur ? uses1 : uses0) & 1u;
+    const bool ok = mbar_wait(&sBar[bcur], parCur, d.waitNs);
+    if (bcur) ++uses1; else ++uses0;
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicCAS(d.err, 0u, kErrTimeout);
+        // the copies this CTA issued must land before its shared memory is released
+        const uint64_t drain = d.waitNs > kDrainNs ? d.waitNs : kDrainNs;
+        mbar_wait(&sBar[bcur], parCur, drain);
+        if (sMisc[2] < nitems) mbar_wait(&sBar[bcur ^ 1u], (bcur ? uses0 : uses1) & 1u, drain);
+      }
+      __syncthreads();
+      return;
+    }
+    const uint32_t E1 = sP1[64], E = E1 + sPM[64], units = (E + 31u) >> 5;
+    const uint32_t* tileBase = sTile + bcur * kItemWords;
+    for (;;) {
+      uint32_t u = 0;
+      if (lane == 0) u = atomicAdd(sMisc + 3, 1u);
+      u = __shfl_sync(kFull, u, 0);
+      if (u >= units) break;
+      uint32_t flat = u * 32u + lane;
+      if (flat >= E) continue;
+      const bool single = flat < E1;
+      const uint32_t* P = single ? sP1 : sPM;
+      if (!single) flat -= E1;
+      uint32_t sp = 0;
+#pragma unroll
+      for (uint32_t step = 32; step; step >>= 1)
+        if (sp + step < 64u && P[sp + step] <= flat) sp += step;
+      const uint32_t e = flat - P[sp];
+      const uint32_t g = sConn[sp];
+      const uint32_t* tile = tileBase + (sp >> 5) * kColWords + (sp & 31u) * 256u;
+      if (single) {  // one nonzero word: 32 AND-counts
+        const uint2 en = __ldcg(e1In + (size_t)g * kServeMaxB + e);
+        const uint32_t b = en.x & 0xFFFFu, w = en.x >> 16, S = en.y;
+        uint32_t* accb = sAcc + ((sp >> 5) * B + b) * accStride;
+#pragma unroll 4
+        for (uint32_t r = 0; r < 32u; r += 4) {
+          const uint4 a = *reinterpret_cast<const uint4*>(tile + w3r_pos(r, w));
+          acc_add4<PACK>(accb, r, branch_term<LIN>(__popc(a.x & S), dthr, bst),
+                         branch_term<LIN>(__popc(a.y & S), dthr, bst), branch_term<LIN>(__popc(a.z & S), dthr, bst),
+                         branch_term<LIN>(__popc(a.w & S), dthr, bst));
+        }
+      } else {  // several nonzero words: counts in registers (words past the third from the spikes)
+        const uint4 en = __ldcg(eMIn + (size_t)g * kServeMaxB + e);
+        const uint32_t b = en.x & 0xFFFFu, nz = (en.x >> 16) & 0xFFu;
+        uint32_t* accb = sAcc + ((sp >> 5) * B + b) * accStride;
+        uint32_t cnt[32];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) cnt[r] = 0u;
+        uint32_t m = nz, k = 0;
+        while (m) {
+          const uint32_t w = (uint32_t)__ffs(m) - 1u;
+          m &= m - 1u;
+          const uint32_t S = k == 0 ? en.y : k == 1 ? en.z : k == 2 ? en.w : __ldcg(spk_prev(bn.tabOff, b) + 8u * g + w);
+          ++k;
+#pragma unroll
+          for (int r = 0; r < 32; r += 4) {
+            const uint4 a = *reinterpret_cast<const uint4*>(tile + w3r_pos(r, w));
+            cnt[r] += __popc(a.x & S); cnt[r + 1] += __popc(a.y & S);
+            cnt[r + 2] += __popc(a.z & S); cnt[r + 3] += __popc(a.w & S);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < 32; r += 4)
+          acc_add4<PACK>(accb, r, branch_term<LIN>(cnt[r], dthr, bst), branch_term<LIN>(cnt[r + 1], dthr, bst),
+                         branch_term<LIN>(cnt[r + 2], dthr, bst), branch_term<LIN>(cnt[r + 3], dthr, bst));
+      }
+    }
+    __syncthreads();
+    // per-neuron and column drives of the item's columns into every trajectory's slot
+    const uint32_t accOff = serve_acc_off(ncol), xOff = 2u * ncol + 2u * d.nactw;
+    if (PACK) {  // the packed counters are the u16 drives: half a warp per (column, trajectory)
+      const uint32_t half = lane >> 4, l16 = lane & 15u;
+      for (uint32_t pp = warp * 2u + half; pp < kRecallCpi * B; pp += nw * 2u) {
+        const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
+        if (col >= ncol) continue;  // uniform over the half warp
+        uint32_t* base = d.slots + (size_t)__ldg(d.btab + bn.tabOff + b).x * d.slotWords;
+        const uint32_t w = sAcc[(colL * B + b) * accStride + l16];
+        __stcg(base + accOff + col * 16u + l16, w);
+        const uint32_t dsum = __reduce_add_sync(half ? 0xFFFF0000u : 0x0000FFFFu, (w & 0xFFFFu) + (w >> 16));
+        if (l16 == 0) __stcg(base + xOff + col, dsum);
+      }
+    } else {
+      for (uint32_t pp = warp; pp < kRecallCpi * B; pp += nw) {
+        const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
+        if (col >= ncol) continue;
+        const uint2 st = __ldg(d.btab + bn.tabOff + b);
+        uint32_t* base = d.slots + (size_t)st.x * d.slotWords;
+        uint32_t a = sAcc[(colL * B + b) * accStride + lane];
+        if (c.facil != 0u && st.y > 0u && ((__ldcg(base + ((st.y - 1u) & 1u) * ncol + col) >> lane) & 1u)) a += c.facil;
+        if (c.acc32) __stcg(base + accOff + col * 32u + lane, a);
+        else __stcg(reinterpret_cast<unsigned short*>(base + accOff) + col * 32u + lane, (unsigned short)a);
+        const uint32_t dsum = __reduce_add_sync(kFull, a);
+        if (lane == 0) __stcg(base + xOff + col, dsum);
+      }
+    }
+    __syncthreads();
+    item = sMisc[2];
+    kbuf ^= 1u;
+  }
+}
+
+size_t serve_batched_smem_bytes(uint32_t packed) {
+  const size_t maxB = packed ? kServeMaxB : kServeMaxB32, stride = packed ? 17 : 33;
+  return (2ull * kItemWords + kRecallCpi * maxB * stride + 64 + 68 + 68 + 16 + 4) * 4;
+}
+
+namespace {
+const void* sb_fn(uint32_t packed, uint32_t lin) {
+  if (packed) return lin ? (const void*)k_serve_batched<true, true> : (const void*)k_serve_batched<true, false>;
+  return lin ? (const void*)k_serve_batched<false, true> : (const void*)k_serve_batched<false, false>;
+}
+}  // namespace
+
+cudaError_t serve_batched_prepare(uint32_t packed) {
+  for (uint32_t lin = 0; lin < 2; ++lin) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(sb_fn(packed, lin), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)serve_batched_smem_bytes(packed));
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_serve_batched(const ServeDev& d, const ServeCfg& c, int sms, cudaStream_t st) {
+  const uint32_t packed = (!c.acc32 && c.facil == 0u) ? 1u : 0u;
+  void* args[] = {(void*)&d, (void*)&c};
+  return cudaLaunchKernel(sb_fn(packed, c.mode != 2u), dim3(sms), dim3(1024), args, serve_batched_smem_bytes(packed), st);
+}
+
+}  // namespace axon

@@ -53,25 +53,30 @@ struct Done {
 struct axon_server {
   std::vector<axon_net*> nets;
   int device = 0, sms = 0;
-  uint32_t ncol = 0, incols = 0, nslots = 0;
+  uint32_t ncol = 0, incols = 0, nslots = 0, capB = 0;
   uint64_t slotCost = 0, fixedCost = 0;  // device bytes per trajectory slot, and fixed
   ServeCfg cfg{};
   size_t emitSmem = 0;
   cudaStream_t stream = nullptr;
-  void* dmem = nullptr;        // slots, tables, done buffer
-  void* hmem = nullptr;        // pinned tick staging
-  void* hdone = nullptr;       // pinned done buffer
+  void* dmem = nullptr;   // slots, entry lists, tables, done buffer, error word
+  void* hmem = nullptr;   // pinned tick staging
+  void* hdone = nullptr;  // pinned done buffer
+  uint32_t* herr = nullptr;  // pinned copy of the error word
   ServeDev dev{};
   size_t stageBytes = 0;
+  uint32_t par = 0;  // tick parity of the entry lists
   std::vector<ServeEntry> entH;  // the tick's tables, built on the server thread
   std::vector<ServeGroup> grpH;
+  std::vector<ServeBNet> bnH;
+  std::vector<uint2> tabH;
   std::vector<uint32_t> cueH;
   std::vector<uint32_t> freeSlots;
 
   std::mutex mu;
   std::condition_variable cv, cvIdle;
-  std::deque<Request> queue;  // by arrival time
-  std::vector<Active> active;
+  std::deque<Request> queue;              // by arrival time
+  std::vector<std::vector<Active>> act;   // per network, in batch-index order
+  size_t nActive = 0;
   std::deque<Done> done;
   bool stop = false;
   axon_status err = AXON_OK;
@@ -113,24 +118,39 @@ axon_status axon_server::start(axon_net* const* ns, uint32_t n, uint64_t memByte
   ncol = n0->ncol;
   incols = n0->cfg.incols;
   sms = n0->sm_count;
+  if (ncol > 8192) return set_error(AXON_EINVAL, "serving supports ncol <= 8192");
   const PresentCfg pc = n0->present_cfg(1, 0, false, 0);  // readout parameters (learn = 0)
   cfg.ncol = ncol; cfg.incols = incols; cfg.dthr = pc.dthr; cfg.boost = pc.boost; cfg.mode = pc.mode;
   cfg.targetCols = pc.targetCols; cfg.k = pc.k; cfg.facil = pc.facil; cfg.topkPar = pc.topkPar;
+  cfg.bst = cfg.mode == 1 ? cfg.boost : 0u;
   // per-neuron drive fits 16 bits unless one neuron's branches can add up past 65535
   const uint64_t maxAcc = (cfg.mode == 2 ? 32ull : 32ull * (256ull + cfg.boost)) + cfg.facil;
   cfg.acc32 = maxAcc > 65535ull ? 1u : 0u;
+  const uint32_t packed = (!cfg.acc32 && cfg.facil == 0u) ? 1u : 0u;
+  capB = packed ? kServeMaxB : kServeMaxB32;
   CKS(cudaSetDevice(device));
+  for (axon_net* x : nets) {  // the batched tile layout of every served network
+    axon_status st = x->ensure_w3b();
+    if (st != AXON_OK) return st;
+    CKS(cudaStreamSynchronize(x->stream));
+  }
+  const uint32_t ngrp = ncol / 8u;
+  // fixed: network table, entry lists of every network, error word, tick tables' fixed part
+  const size_t listBytes = al(2ull * ngrp * kServeMaxB * 8) + al(2ull * ngrp * kServeMaxB * 16) + al(4ull * ngrp * 4);
+  const uint64_t fixed = al(n * sizeof(ServeNet)) + n * listBytes + 256 + 1024 + al(n * sizeof(ServeGroup)) +
+                         al(n * sizeof(ServeBNet));
   // one slot: its buffers, its share of the done buffer and of the tick tables
   const size_t slotBytes = (size_t)serve_slot_words(ncol, cfg.acc32) * 4;
-  const size_t perSlot = slotBytes + (size_t)ncol * 4 + sizeof(ServeEntry) + sizeof(ServeGroup) + (size_t)incols * 4;
-  const uint64_t fixed = al(n * sizeof(ServeNet)) + 4 * 256 + al(n * sizeof(ServeGroup));
+  const size_t perSlot = slotBytes + (size_t)ncol * 4 + sizeof(ServeEntry) + sizeof(ServeGroup) + sizeof(uint2) +
+                         (size_t)incols * 4;
   if (memBytes <= fixed + perSlot) return set_error(AXON_EINVAL, "memory budget below one trajectory slot");
   nslots = (uint32_t)std::min<uint64_t>((memBytes - fixed) / (perSlot + 64), 1u << 16);
   slotCost = perSlot + 64;
   fixedCost = fixed;
-  stageBytes = 256 + al(nslots * sizeof(ServeEntry)) + al((nslots + n) * sizeof(ServeGroup)) +
-               al((size_t)nslots * incols * 4);
-  const size_t netsOff = 0, slotsOff = al(n * sizeof(ServeNet)), stageOff = slotsOff + al((size_t)nslots * slotBytes),
+  stageBytes = 1024 + al(nslots * sizeof(ServeEntry)) + al((nslots + n) * sizeof(ServeGroup)) +
+               al(n * sizeof(ServeBNet)) + al(nslots * sizeof(uint2)) + al((size_t)nslots * incols * 4);
+  const size_t netsOff = 0, listsOff = al(n * sizeof(ServeNet)), errOff = listsOff + n * listBytes,
+               slotsOff = errOff + 256, stageOff = slotsOff + al((size_t)nslots * slotBytes),
                doneOff = stageOff + al(stageBytes), total = doneOff + al((size_t)nslots * ncol * 4);
   if (cudaMalloc(&dmem, total) != cudaSuccess) {
     cudaGetLastError();
@@ -139,22 +159,36 @@ axon_status axon_server::start(axon_net* const* ns, uint32_t n, uint64_t memByte
   }
   CKS(cudaMallocHost(&hmem, stageBytes));
   CKS(cudaMallocHost(&hdone, (size_t)nslots * ncol * 4));
+  CKS(cudaMallocHost((void**)&herr, 64));
   CKS(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   for (auto& e : ev) CKS(cudaEventCreate(&e));
   char* b = (char*)dmem;
+  CKS(cudaMemsetAsync(b + listsOff, 0, n * listBytes + 256, stream));  // list lengths and error word start at zero
   std::vector<ServeNet> hn(n);
-  for (uint32_t i = 0; i < n; ++i) hn[i] = ServeNet{nets[i]->d.W3, nets[i]->d.conn};
+  for (uint32_t i = 0; i < n; ++i) {
+    char* L = b + listsOff + i * listBytes;
+    hn[i].W3 = nets[i]->d.W3;
+    hn[i].conn = nets[i]->d.conn;
+    hn[i].W3R = nets[i]->w3b;
+    hn[i].ent1 = (uint2*)L;
+    hn[i].entM = (uint4*)(L + al(2ull * ngrp * kServeMaxB * 8));
+    hn[i].ecnt = (uint32_t*)(L + al(2ull * ngrp * kServeMaxB * 8) + al(2ull * ngrp * kServeMaxB * 16));
+  }
   CKS(cudaMemcpyAsync(b + netsOff, hn.data(), n * sizeof(ServeNet), cudaMemcpyHostToDevice, stream));
   dev.nets = (const ServeNet*)(b + netsOff);
   dev.slots = (uint32_t*)(b + slotsOff);
-  dev.counts = (const uint32_t*)(b + stageOff);  // entries, groups and cues follow, packed per tick
+  dev.counts = (const uint32_t*)(b + stageOff);  // the tick's tables follow, packed per tick
   dev.doneBuf = (uint32_t*)(b + doneOff);
+  dev.err = (uint32_t*)(b + errOff);
   dev.slotWords = serve_slot_words(ncol, cfg.acc32);
   dev.nactw = serve_nactw(ncol);
+  dev.waitNs = n0->wait_ns;
   emitSmem = serve_emit_smem_bytes(ncol, incols);
   CKS(serve_prepare(emitSmem));
+  CKS(serve_batched_prepare(packed));
   CKS(cudaStreamSynchronize(stream));
   for (uint32_t s = nslots; s-- > 0;) freeSlots.push_back(s);
+  act.assign(n, {});
   th = std::thread([this] { loop(); });
   return AXON_OK;
 }
@@ -170,6 +204,7 @@ axon_server::~axon_server() {
   if (dmem) cudaFree(dmem);
   if (hmem) cudaFreeHost(hmem);
   if (hdone) cudaFreeHost(hdone);
+  if (herr) cudaFreeHost(herr);
   for (auto& e : ev)
     if (e) cudaEventDestroy(e);
   if (stream) cudaStreamDestroy(stream);
@@ -182,7 +217,7 @@ void axon_server::loop() {
       std::unique_lock<std::mutex> g(mu);
       for (;;) {
         if (stop || err != AXON_OK) return;
-        if (!active.empty()) break;
+        if (nActive) break;
         if (!queue.empty()) {
           const double wait = queue.front().arrive - now_s();
           if (wait <= 0) break;
@@ -202,114 +237,145 @@ void axon_server::loop() {
 }
 
 axon_status axon_server::tick() {
-  // admission: arrived requests, in arrival order, into free slots
-  std::vector<Active> admitted;
+  // admission: arrived requests, in arrival order, into free slots, while the request's
+  // network has room in its batch
   {
     std::lock_guard<std::mutex> g(mu);
     const double t = now_s();
-    while (!queue.empty() && !freeSlots.empty() && queue.front().arrive <= t) {
+    while (!queue.empty() && !freeSlots.empty() && queue.front().arrive <= t && act[queue.front().net].size() < capB) {
       Active a{freeSlots.back(), 0u, std::move(queue.front())};
       freeSlots.pop_back();
       queue.pop_front();
       a.req.admit = t;
-      admitted.push_back(std::move(a));
+      act[a.req.net].push_back(std::move(a));
+      ++nActive;
     }
   }
-  for (auto& a : admitted) active.push_back(std::move(a));
-  if (active.empty()) return AXON_OK;
-  // the tick's tables: entries grouped by network, up to kServeGroup per group
-  std::sort(active.begin(), active.end(), [](const Active& x, const Active& y) {
-    return x.req.net != y.req.net ? x.req.net < y.req.net : x.slot < y.slot;
-  });
-  std::vector<ServeEntry>& ent = entH;
-  std::vector<ServeGroup>& grp = grpH;
-  std::vector<uint32_t>& cue = cueH;
-  ent.clear();
-  grp.clear();
-  cue.clear();
+  if (nActive == 0) return AXON_OK;
+  // the tick's tables: every network's trajectories in batch-index order; a network with
+  // many of them is advanced by the batched kernel, the others by the gather kernel
+  entH.clear();
+  grpH.clear();
+  bnH.clear();
+  tabH.clear();
+  cueH.clear();
   uint32_t ndone = 0;
-  for (const Active& a : active) {
-    ServeEntry e{};
-    e.slot = a.slot;
-    e.net = a.req.net;
-    e.tloc = a.tloc;
-    e.clamp = a.req.clamp;
-    if (a.tloc < a.req.clamp) {
-      e.ncue = (uint32_t)a.req.cue.size();
-      e.cueOff = (uint32_t)cue.size();
-      cue.insert(cue.end(), a.req.cue.begin(), a.req.cue.end());
+  for (uint32_t n = 0; n < (uint32_t)act.size(); ++n) {
+    const std::vector<Active>& A = act[n];
+    if (A.empty()) continue;
+    const bool batched = A.size() >= kServeBatchMin;
+    if (batched) bnH.push_back(ServeBNet{n, (uint32_t)A.size(), (uint32_t)tabH.size(), 0u});
+    uint32_t cont = 0;
+    for (const Active& a : A) {
+      ServeEntry e{};
+      e.slot = a.slot;
+      e.net = n;
+      e.tloc = a.tloc;
+      e.clamp = a.req.clamp;
+      if (a.tloc < a.req.clamp) {
+        e.ncue = (uint32_t)a.req.cue.size();
+        e.cueOff = (uint32_t)cueH.size();
+        cueH.insert(cueH.end(), a.req.cue.begin(), a.req.cue.end());
+      }
+      const bool last = a.tloc + 1 == a.req.steps;
+      e.done = last ? ndone++ : 0xFFFFFFFFu;
+      e.nextIdx = last ? 0xFFFFFFFFu : cont++;
+      if (batched) {
+        tabH.push_back(make_uint2(a.slot, a.tloc));
+      } else {
+        if (grpH.empty() || grpH.back().net != n || grpH.back().n == kServeGroup) {
+          ServeGroup gr{};
+          gr.net = n;
+          grpH.push_back(gr);
+        }
+        grpH.back().e[grpH.back().n++] = (uint32_t)entH.size();
+      }
+      entH.push_back(e);
     }
-    e.done = (a.tloc + 1 == a.req.steps) ? ndone++ : 0xFFFFFFFFu;
-    if (grp.empty() || grp.back().net != e.net || grp.back().n == kServeGroup) {
-      ServeGroup g{};
-      g.net = e.net;
-      grp.push_back(g);
-    }
-    grp.back().e[grp.back().n++] = (uint32_t)ent.size();
-    ent.push_back(e);
   }
-  const uint32_t ne = (uint32_t)ent.size(), ng = (uint32_t)grp.size(), nc = (uint32_t)cue.size();
-  // one upload: [counts][entries][groups][cue columns], packed to what this tick uses
-  const size_t oEnt = 256, oGrp = oEnt + al(ne * sizeof(ServeEntry)), oCue = oGrp + al(ng * sizeof(ServeGroup)),
+  const uint32_t ne = (uint32_t)entH.size(), ng = (uint32_t)grpH.size(), nb = (uint32_t)bnH.size(),
+                 nc = (uint32_t)cueH.size();
+  const uint32_t nip = (ncol + kRecallCpi - 1) / kRecallCpi;
+  // one upload: [counts, work counter][entries][groups][batched networks][their table][cues]
+  const size_t oEnt = 256, oGrp = oEnt + al(ne * sizeof(ServeEntry)), oBn = oGrp + al(ng * sizeof(ServeGroup)),
+               oTab = oBn + al(nb * sizeof(ServeBNet)), oCue = oTab + al(tabH.size() * sizeof(uint2)),
                bytes = oCue + (size_t)nc * 4;
   char* h = (char*)hmem;
   uint32_t* cnt = (uint32_t*)h;
   cnt[0] = ne;
   cnt[1] = ng;
-  std::memcpy(h + oEnt, ent.data(), ne * sizeof(ServeEntry));
-  std::memcpy(h + oGrp, grp.data(), ng * sizeof(ServeGroup));
-  if (nc) std::memcpy(h + oCue, cue.data(), (size_t)nc * 4);
+  cnt[2] = nb;
+  cnt[3] = nb * nip;
+  cnt[4] = 0u;  // work counter of the batched kernel
+  std::memcpy(h + oEnt, entH.data(), ne * sizeof(ServeEntry));
+  if (ng) std::memcpy(h + oGrp, grpH.data(), ng * sizeof(ServeGroup));
+  if (nb) std::memcpy(h + oBn, bnH.data(), nb * sizeof(ServeBNet));
+  if (!tabH.empty()) std::memcpy(h + oTab, tabH.data(), tabH.size() * sizeof(uint2));
+  if (nc) std::memcpy(h + oCue, cueH.data(), (size_t)nc * 4);
   ServeDev td = dev;
   char* ds = (char*)dev.counts;
+  td.work = (uint32_t*)(ds + 16);
   td.ent = (const ServeEntry*)(ds + oEnt);
   td.grp = (const ServeGroup*)(ds + oGrp);
+  td.bnets = (const ServeBNet*)(ds + oBn);
+  td.btab = (const uint2*)(ds + oTab);
   td.cues = (const uint32_t*)(ds + oCue);
+  td.par = par;
   CKS(cudaMemcpyAsync(ds, h, bytes, cudaMemcpyHostToDevice, stream));
   CKS(cudaEventRecord(ev[0], stream));
-  CKS(launch_serve_tick(td, cfg, sms, emitSmem, stream, ev[1]));
+  CKS(launch_serve_drive(td, cfg, sms, ng > 0, nb > 0, stream));
+  CKS(cudaEventRecord(ev[1], stream));
+  CKS(launch_serve_emit(td, cfg, sms, emitSmem, stream, (uint32_t)nets.size()));
   CKS(cudaEventRecord(ev[2], stream));
   if (ndone) CKS(cudaMemcpyAsync(hdone, dev.doneBuf, (size_t)ndone * ncol * 4, cudaMemcpyDeviceToHost, stream));
+  CKS(cudaMemcpyAsync(herr, dev.err, 4, cudaMemcpyDeviceToHost, stream));
   CKS(cudaStreamSynchronize(stream));
   const double t = now_s();
+  if (herr[0] != 0u) return set_error(AXON_ETIMEOUT, "a copy wait timed out in the serving kernel");
   float msDrive = 0.f, msEmit = 0.f;
   CKS(cudaEventElapsedTime(&msDrive, ev[0], ev[1]));
   CKS(cudaEventElapsedTime(&msEmit, ev[1], ev[2]));
-  // retire finished trajectories, advance the others
-  std::vector<Active> keep;
-  keep.reserve(active.size());
+  par ^= 1u;
+  // retire finished trajectories; the others keep their order (their next batch indices)
   std::vector<Done> fin;
   std::vector<uint32_t> freed;
-  for (uint32_t i = 0; i < ne; ++i) {
-    Active& a = active[i];
-    if (ent[i].done != 0xFFFFFFFFu) {
-      Done d;
-      d.r.tag = a.req.tag;
-      d.r.net = a.req.net;
-      d.r.steps = a.req.steps;
-      d.r.arrive_s = a.req.arrive;
-      d.r.admit_s = a.req.admit;
-      d.r.done_s = t;
-      const uint32_t* src = (const uint32_t*)hdone + (size_t)ent[i].done * ncol;
-      d.spk.assign(src, src + ncol);
-      fin.push_back(std::move(d));
-      freed.push_back(a.slot);
-    } else {
-      ++a.tloc;
-      keep.push_back(std::move(a));
+  uint32_t ei = 0;
+  for (std::vector<Active>& A : act) {
+    std::vector<Active> keep;
+    keep.reserve(A.size());
+    for (Active& a : A) {
+      const ServeEntry& e = entH[ei++];
+      if (e.done != 0xFFFFFFFFu) {
+        Done d;
+        d.r.tag = a.req.tag;
+        d.r.net = a.req.net;
+        d.r.steps = a.req.steps;
+        d.r.arrive_s = a.req.arrive;
+        d.r.admit_s = a.req.admit;
+        d.r.done_s = t;
+        const uint32_t* src = (const uint32_t*)hdone + (size_t)e.done * ncol;
+        d.spk.assign(src, src + ncol);
+        fin.push_back(std::move(d));
+        freed.push_back(a.slot);
+      } else {
+        ++a.tloc;
+        keep.push_back(std::move(a));
+      }
     }
+    A.swap(keep);
   }
-  active.swap(keep);
   {
     std::lock_guard<std::mutex> g(mu);
     for (auto& d : fin) done.push_back(std::move(d));
     for (uint32_t s : freed) freeSlots.push_back(s);
+    nActive -= fin.size();
     ++ticks;
     driveS += msDrive * 1e-3;
     emitS += msEmit * 1e-3;
     sumActive += ne;
     maxActive = std::max<uint64_t>(maxActive, ne);
     completed += fin.size();
-    if (active.empty() && queue.empty()) cvIdle.notify_all();
+    if (nActive == 0 && queue.empty()) cvIdle.notify_all();
   }
   return AXON_OK;
 }
