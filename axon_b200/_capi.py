@@ -64,7 +64,7 @@ class MultiResult(C.Structure):
 class MultiReport(C.Structure):
     _fields_ = [("gpu_ms", C.c_double), ("tune_ms", C.c_double), ("steps", C.c_uint64), ("train_steps", C.c_uint64),
                 ("slots", C.c_uint32), ("threads", C.c_uint32), ("tiles", C.c_uint32), ("grid", C.c_uint32),
-                ("graph", C.c_uint32), ("tried", C.c_uint32)]
+                ("graph", C.c_uint32), ("tried", C.c_uint32), ("w3_tiles", C.c_uint64), ("learn_tasks", C.c_uint64)]
 
 
 MULTI_ONE_LAUNCH, MULTI_PLAIN = 0, 1

@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(NT, 1) k_multi(MultiDev m, MultiCfg c) {
   uint32_t* bar = m.bars + slot * 32u;
   if (tid == 0) { sFlag[1] = 0u; sFlag[2] = 0u; }
   uint32_t gstep = 0;   // slot-wide step counter: barrier epoch and exchange parity
+  uint32_t nTiles = 0;  // W3 tiles this warp read (summed into m.work at the end)
   uint32_t thPrev = 0;  // last threshold: a starting guess for the next selection
 
   for (uint32_t qi = S.q0; qi < S.q1; ++qi) {
@@ -143,6 +144,7 @@ __global__ void __launch_bounds__(NT, 1) k_multi(MultiDev m, MultiCfg c) {
             if (cc + nwS < ncol) cnNext = __ldg(conn + (cc + nwS) * kNslot + lane);
             const uint32_t bsrc = useBias ? __ldcg(biasG + cc * 32u + lane) : 0u;
             uint32_t active = __ballot_sync(kFull, (sActIn[cn >> 5] >> (cn & 31u)) & 1u);
+            nTiles += __popc(active);
             uint32_t a = 0, b2 = 0;
             const uint4* Wt = W3 + (size_t)cc * kNslot * kTileU4 + lane;
             while (active) {
@@ -290,6 +292,7 @@ __global__ void __launch_bounds__(NT, 1) k_multi(MultiDev m, MultiCfg c) {
               }
               __syncthreads();
               const uint32_t ntask = sFlag[2];
+              if (tid == 0) atomicAdd(m.work + 1, (unsigned long long)ntask);
               for (uint32_t k = warp; k < ntask; k += wpb) {
                 const uint32_t tk = sTask[k], j = tk >> 5, s = tk & 31u;
                 const uint32_t cc = sColC[j];
@@ -369,6 +372,7 @@ __global__ void __launch_bounds__(NT, 1) k_multi(MultiDev m, MultiCfg c) {
       __syncthreads();
     }
   }
+  if (lane == 0 && nTiles) atomicAdd(m.work, (unsigned long long)nTiles);
 }
 
 // ---------------------------------------------------------------- launch helpers

@@ -41,6 +41,7 @@ struct MultiDev {
   const uint32_t* queue;    // network indices, grouped by slot
   uint32_t* bars;           // [nslots * 32] barrier counters (one 128-byte line each), zeroed
   uint32_t* err;            // device error word
+  unsigned long long* work; // [0] W3 tiles read by the drive, [1] learning tasks (branch read-modify-writes)
   uint32_t nslots, pad;
 };
 

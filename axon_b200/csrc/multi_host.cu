@@ -117,6 +117,7 @@ class MultiRun {
   char* base_ = nullptr;
   size_t ctlOff_ = 0;  // MultiNet / slots / queue / bars / err / plain-path scratch region
   MultiCfg cfg_{};
+  unsigned long long lastWork_[2] = {0, 0};  // tiles read, learning tasks of the last launch
 
   uint32_t* dev(size_t off) const { return (uint32_t*)(base_ + off); }
   axon_status plan(const uint32_t* seeds, const uint32_t* nstim);
@@ -290,6 +291,7 @@ axon_status MultiRun::launch(const Shape& sh, const std::vector<std::vector<uint
   m.queue = dQueue;
   m.bars = dBars;
   m.err = dErr;
+  m.work = reinterpret_cast<unsigned long long*>(dErr + 4);  // 16 bytes into the error word's 64-byte line
   m.nslots = S;
   MultiCfg c = cfg_;
   c.maxCpw = max_cpw(ncta, sh.threads);
@@ -304,7 +306,7 @@ axon_status MultiRun::launch(const Shape& sh, const std::vector<std::vector<uint
 
   auto body = [&]() -> cudaError_t {
     cudaError_t e = cudaMemsetAsync(dBars, 0, (size_t)S * 32 * 4, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(dErr, 0, 4, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dErr, 0, 32, st);  // error word and work counters
     if (e == cudaSuccess) e = launch_multi(m, c, shp, st);
     return e;
   };
@@ -341,8 +343,10 @@ axon_status MultiRun::launch(const Shape& sh, const std::vector<std::vector<uint
   if (exec) cudaGraphExecDestroy(exec);
   if (es != cudaSuccess) return cuda_fail(es, "multi-network launch");
   CK(cudaEventElapsedTime(ms, net0_->ev0, net0_->ev1));
-  uint32_t err = 0;
-  CK(cudaMemcpy(&err, dErr, 4, cudaMemcpyDeviceToHost));
+  uint32_t words[8] = {0};
+  CK(cudaMemcpy(words, dErr, 32, cudaMemcpyDeviceToHost));
+  const uint32_t err = words[0];
+  std::memcpy(lastWork_, words + 4, 16);
   if (err)
     return set_error(AXON_ETIMEOUT, "grid wait timed out in the multi-network kernel (code " + std::to_string(err) + ")");
   return AXON_OK;
@@ -574,6 +578,8 @@ axon_status MultiRun::run(const uint32_t* seeds, const uint32_t* nstim, axon_mul
     R.tiles = (uint32_t)sh.tiles;
     R.grid = std::accumulate(ncta.begin(), ncta.end(), 0u);
     R.graph = g ? 1u : 0u;
+    R.w3_tiles = lastWork_[0];
+    R.learn_tasks = lastWork_[1];
   }
   R.gpu_ms = ms;
   for (uint32_t i = 0; i < n_; ++i) {

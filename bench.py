@@ -113,6 +113,13 @@ def bench_multi(dev: int, nnets: int = 25, epochs: int = EPOCHS) -> dict:
             for r in json.loads((ROOT / "tests" / "golden" / "published.json").read_text())["table1"]}
     rows = {L: printed(res_m[i]) for i, (s, L) in enumerate(zip(seeds, loads)) if s == 0}
     steps = rep_m["steps"]
+    # algorithmic HBM bytes of the launch: W3 tiles read by the drive, branch updates of
+    # the learning rule (4 planes read + written), conn and spikes per step, bias per
+    # learning step
+    alg = (1024.0 * rep_m["w3_tiles"] + 8192.0 * rep_m["learn_tasks"] + steps * (512 + 16) * 1024.0
+           + rep_m["train_steps"] * 1024.0 * 1024.0)
+    hbm_peak, pk = peaks()
+    achieved = alg / (rep_m["gpu_ms"] / 1e3) / 1e9
     return {"workload": f"{len(nets)} networks (seeds 0-4 x loads 12,24,36,48,60), config C, {epochs} epochs + readouts",
             "networks": len(nets), "network_steps": steps, "learning_steps": rep_m["train_steps"],
             "one_launch_ms": rep_m["gpu_ms"], "plain_ms": rep_p["gpu_ms"],
@@ -120,6 +127,10 @@ def bench_multi(dev: int, nnets: int = 25, epochs: int = EPOCHS) -> dict:
             "plain_steps_per_s": steps / (rep_p["gpu_ms"] / 1e3), "speedup_vs_plain": rep_p["gpu_ms"] / rep_m["gpu_ms"],
             "shape": {k: rep_m[k] for k in ("slots", "threads", "tiles", "grid", "graph", "tried")},
             "tune_ms": rep_m["tune_ms"], "bit_exact_vs_plain": True,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "peak_kind": pk, "w3_tiles": rep_m["w3_tiles"], "learn_tasks": rep_m["learn_tasks"],
+                         "note": "algorithmic bytes = 1 KiB per W3 tile read + 8 KiB per learning branch update + "
+                                 "conn/spikes per step + bias per learning step"},
             "seed0_rows": rows,
             "seed0_rows_equal_published_table1": epochs == EPOCHS and all(rows[L] == gold[L] for L in rows)}
 
@@ -268,6 +279,14 @@ class ClockSampler:
         reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 2 + i and r[2 + i] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from its committed ncu capture (profiles/), or None."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    return json.loads(p.read_text()).get(kernel, {}).get("dram_bytes_per_launch")
 
 
 def peaks() -> tuple[float, str]:
@@ -470,7 +489,7 @@ def main() -> None:
                    "train_s": round(train_s, 2), "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "peak_kind": peak_kind,
+                     "traffic": measured_traffic("k_recall"), "peak_kind": peak_kind,
                      "note": "algorithmic bytes = 45 x (W3 128 MiB + u16 drive slab + spike vectors); the kernel is "
                              "issue-bound, see profiles/"},
         "cpu_baseline": cpu,

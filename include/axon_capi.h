@@ -257,6 +257,8 @@ typedef struct axon_multi_report {
   uint32_t slots, threads, tiles, grid; /* shape used (slots = 0 for the plain path) */
   uint32_t graph;       /* 1 when the launch ran as a CUDA graph */
   uint32_t tried;       /* candidate shapes timed */
+  uint64_t w3_tiles;    /* W3 tiles (1 KiB each) the drive read: (column, branch) pairs with a spiking group */
+  uint64_t learn_tasks; /* branch updates of k_learn (W0..W3 tiles read and written, 8 KiB each) */
 } axon_multi_report;
 
 axon_status axon_multi_train(axon_net* const* nets, uint32_t n, const uint32_t* seeds, const uint32_t* nstim,
