@@ -136,6 +136,24 @@ axon_status axon_bstest(int device, uint32_t op, uint32_t lo, uint32_t hi, uint3
   return AXON_OK;
 }
 
+axon_status axon_clone(const axon_net* src, axon_net** out) {
+  if (!src || !out) return fail(AXON_EINVAL, "null argument");
+  *out = nullptr;
+  axon_net* n = new axon_net();
+  axon_status st = n->create(src->cfg, src->device);
+  if (st == AXON_OK) st = n->clone_from(*src);
+  if (st != AXON_OK) { delete n; return st; }
+  *out = n;
+  return AXON_OK;
+}
+
+axon_status axon_profile_present(axon_net* net, const uint32_t* stim, uint32_t T, uint32_t clamp_steps, int learn,
+                                 uint32_t use_bias, double out[6]) {
+  if (!net || !stim || !out) return fail(AXON_EINVAL, "null argument");
+  if (use_bias > 2) return fail(AXON_EINVAL, "use_bias must be 0, 1 or 2");
+  return net->profile_present(stim, T, clamp_steps, learn != 0, use_bias, out);
+}
+
 axon_status axon_set_wait_limit(axon_net* net, uint64_t ns) {
   if (!net || ns == 0) return fail(AXON_EINVAL, "bad argument");
   net->wait_ns = ns;

@@ -46,6 +46,7 @@ axon_status axon_net::create(const axon_cfg& c, int dev) {
                             64ull * ncol, 16, 2ull * ncol, 2ull * ncol, 64, 64};
   uint64_t total = 4 * plane_words * 4;
   for (uint64_t w : small) total += (w * 4 + 255) & ~255ull;
+  base_bytes = total;
   if (cudaMalloc(&base, total) != cudaSuccess) {
     cudaGetLastError();
     base = nullptr;
@@ -333,5 +334,56 @@ axon_status axon_net::wdiag(const uint32_t* memb, const uint32_t* asmSpk, uint32
   CK(launch_wdiag(d, ncol, dm, da, nstim, cfg.inbr, sel, dh, stream));
   CK(cudaMemcpyAsync(hist48, dh, 48 * 4, cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
+  return AXON_OK;
+}
+
+axon_status axon_net::profile_present(const uint32_t* stim, uint32_t T, uint32_t clampSteps, bool learn,
+                                      uint32_t useBias, double out[6]) {
+  if (!initialized) return set_error(AXON_ESTATE, "present before init");
+  if (T == 0 || T > 64) return set_error(AXON_EINVAL, "T must be in 1..64 (hist holds 64 steps)");
+  CK(cudaSetDevice(device));
+  DevTmp tmp;
+  const size_t nst = (size_t)T * shape.grid * 5;
+  CK(cudaMalloc(&tmp.p, nst * 8));
+  std::memcpy(hstim, stim, (size_t)ncol * 4);
+  CK(cudaMemcpyAsync(d.stim, hstim, (size_t)ncol * 4, cudaMemcpyHostToDevice, stream));
+  CK(cudaMemsetAsync(d.stats, 0, 1024 * 4, stream));
+  CK(cudaMemsetAsync(d.bar, 0, 4, stream));
+  CK(cudaMemsetAsync(tmp.p, 0, nst * 8, stream));
+  NetDev dd = d;
+  dd.prof = (unsigned long long*)tmp.p;
+  const PresentCfg pc = present_cfg(T, clampSteps, learn, useBias);
+  if (learn) w3b_valid = false;
+  CK(cudaEventRecord(ev0, stream));
+  CK(launch_present(dd, pc, shape, stream));
+  CK(cudaEventRecord(ev1, stream));
+  axon_status st = check_device_error();
+  if (st != AXON_OK) return st;
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ev0, ev1));
+  std::vector<unsigned long long> h(nst);
+  CK(cudaMemcpy(h.data(), tmp.p, nst * 8, cudaMemcpyDeviceToHost));
+  // per phase: mean over CTAs of each CTA's time in it, summed over the steps
+  double ph[4] = {0, 0, 0, 0}, stepT = 0;
+  for (uint32_t t = 0; t < T; ++t) {
+    for (int b = 0; b < shape.grid; ++b) {
+      const unsigned long long* s = h.data() + ((size_t)t * shape.grid + b) * 5;
+      for (int k = 0; k < 4; ++k) ph[k] += (double)(s[k + 1] - s[k]);
+      stepT += (double)(s[4] - s[0]);
+    }
+  }
+  for (int k = 0; k < 4; ++k) out[k] = ph[k] / shape.grid / T / 1e3;  // us per step
+  out[4] = stepT / shape.grid / T / 1e3;
+  out[5] = ms;
+  return AXON_OK;
+}
+
+axon_status axon_net::clone_from(const axon_net& src) {
+  if (!src.initialized) return set_error(AXON_ESTATE, "clone before init");
+  CK(cudaSetDevice(device));
+  CK(cudaMemcpyAsync(base, src.base, base_bytes, cudaMemcpyDeviceToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  initialized = true;
+  w3b_valid = false;
   return AXON_OK;
 }

@@ -35,6 +35,7 @@ struct axon_net {
   uint64_t plane_words = 0;
   axon::NetDev d{};
   void* base = nullptr;        // one device allocation for all buffers
+  size_t base_bytes = 0;
   uint32_t* hstim = nullptr;   // pinned staging for the clamp pattern
   uint32_t* hscratch = nullptr;  // pinned staging for small reads (error word)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -48,6 +49,12 @@ struct axon_net {
   axon_status init(uint32_t seed);
   axon_status present(const uint32_t* stim, uint32_t T, uint32_t clampSteps, bool learn, bool freeze,
                       uint32_t useBias, double* msPerStep);
+  // one presentation with device-timer stamps at every phase boundary: out = us per step of
+  // drive + k-of-32, grid barrier, threshold + emit, records + bias + learning, the whole
+  // step, then the launch in ms
+  axon_status profile_present(const uint32_t* stim, uint32_t T, uint32_t clampSteps, bool learn, uint32_t useBias,
+                              double out[6]);
+  axon_status clone_from(const axon_net& src);  // same configuration: copies every device buffer
   uint64_t buf_words(axon_buf which) const;
   uint32_t* buf_ptr(axon_buf which) const;
   axon_status read(axon_buf which, uint32_t* host, uint64_t words);

@@ -87,6 +87,9 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
     const uint32_t phase = (!c.learn || !c.contrast) ? 0u
                            : (clamp ? 1u : (((t - c.clampSteps) % c.ltdEvery == 0u) ? 2u : 3u));
 
+    // per-phase device timer stamps of the profile mode (thread 0 of every CTA)
+    unsigned long long* stamp = d.prof ? d.prof + ((size_t)t * gridDim.x + blockIdx.x) * 5u : nullptr;
+    if (stamp && tid == 0) stamp[0] = globaltimer_ns();
     // ---------------- phase A: drive (k_drive, src/axon.mm:150-190) + ungated k-WTA
     // The owner warp walks its column's non-silent branches four at a time, so four W3
     // tiles (2 x 512 B each) are in flight per warp; spikes come from shared memory.
@@ -136,7 +139,12 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
       }
     }
 
+    if (stamp) {
+      __syncthreads();
+      if (tid == 0) stamp[1] = globaltimer_ns();
+    }
     if (!grid_barrier(d.bar, d.err, gridDim.x + c.missing, t, c.waitNs, sFlag)) return;
+    if (stamp && tid == 0) stamp[2] = globaltimer_ns();
 
     // ---------------- phase B: column threshold (k_topk) and the full spike vector
     // drives and ballots come from L2 by asynchronous copies; the ballots keep arriving
@@ -158,6 +166,7 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
     __syncthreads();
     if (blockIdx.x == 0 && tid == 0) { d.theta[0] = theta; d.theta[1] = 0u; }
 
+    if (stamp && tid == 0) stamp[3] = globaltimer_ns();
     // ---------------- phase C: own-column records, bias and learning
 #pragma unroll
     for (int i = 0; i < CPW; ++i) {
@@ -267,6 +276,7 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
       if (tid == 0) sFlag[1] = 0u;
     }
     __syncthreads();  // sOut / sActOut complete before the next step reads them
+    if (stamp && tid == 0) stamp[4] = globaltimer_ns();
   }
 
   // ---------------- final state, as the reference's buffers hold it after present()

@@ -14,6 +14,7 @@ struct NetDev {
   uint32_t *xdrive, *xball;  // 2 x ncol exchange slots (step parity) for drives / ungated ballots
   uint32_t *bar, *err;       // grid barrier counter, device error word
   uint32_t* finalOut;        // optional copy of the last step's spikes (recall), or null
+  unsigned long long* prof;  // optional phase timestamps [T][grid][5] (device timer, ns), or null
 };
 
 // Everything one presentation needs (the reference's Params block, resolved for a

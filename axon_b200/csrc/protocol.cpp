@@ -387,6 +387,28 @@ int Session::run() {
     printf("  cue  |  CLAMPED ref: self  other  margin  |  FREE ref: self  other  margin\n");
   }
 
+  if (A.profile) {  // src/axon.mm:1161-1256: one learning presentation of pattern 0, timed per phase
+    axon_net* pn = nullptr;
+    ok(axon_clone(net, &pn), "axon_clone");  // on a copy: profiling changes no weight of the run
+    const uint32_t* w = clamp_words(0, 1.0, 5555);
+    double o[6] = {0, 0, 0, 0, 0, 0};
+    const auto t0 = std::chrono::steady_clock::now();
+    const axon_status st = axon_profile_present(pn, w, T, CLAMP, 1, 2, o);
+    const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / T;
+    axon_destroy(pn);
+    ok(st, "axon_profile_present");
+    const char* rows[4] = {"drive + k-of-32 (k_drive)", "grid barrier", "threshold + emit (k_topk, k_emit)",
+                           "records, bias, learn (k_bias, k_learn)"};
+    printf("\n============= PER-PHASE GPU PROFILE (device timer, one persistent launch) =============\n");
+    printf("  %u timesteps, cue %u steps, learning ON, on a copy of the network\n", T, CLAMP);
+    printf("  %-40s %10s %10s\n", "phase", "us/step", "% of step");
+    for (int k = 0; k < 4; ++k) printf("  %-40s %10.1f %10.1f\n", rows[k], o[k], o[4] > 0 ? 100.0 * o[k] / o[4] : 0.0);
+    printf("  %-40s %10.1f %10.1f\n", "TOTAL", o[4], 100.0);
+    printf("  launch %.3f ms/step | wall %.3f ms/step\n", o[5] / T, wall);
+    printf("  the five kernels run fused in one launch: a per-kernel ablation does not apply\n");
+    printf("========================================================================================\n");
+  }
+
   // STEP A1: in-degree and winner identity, src/axon.mm:1343-1409
   std::vector<uint32_t> indeg(n);
   ok(axon_indeg(net, indeg.data()), "axon_indeg");
@@ -900,7 +922,6 @@ CliArgs CliArgs::parse(int argc, char** argv) {
 }
 
 std::string CliArgs::check() const {
-  if (profile) return "profile=1 (per-stage Metal timestamps and their weight-mutating replay) is not supported";
   if (T == 0 || T > 64) return "T must be in 1..64";
   if (stim == 0) return "stim must be >= 1";
   if (stimcols > incols) return "stimcols must be <= incols";

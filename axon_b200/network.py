@@ -65,6 +65,24 @@ class Network:
                                      C.byref(ms)))
         return ms.value
 
+    def clone(self) -> "Network":
+        """A second network with a copy of every device buffer of this one."""
+        other = Network.__new__(Network)
+        other.cfg, other.ncol, other.n = self.cfg, self.ncol, self.n
+        h = C.c_void_p()
+        A.check(A.lib().axon_clone(self._h, C.byref(h)))
+        other._h = h
+        return other
+
+    def profile_present(self, stim: np.ndarray, T: int, clamp_steps: int, learn: bool = True,
+                        use_bias: int = 2) -> dict:
+        """One presentation timed per phase with the device timer (us per step)."""
+        stim = np.ascontiguousarray(stim, dtype=np.uint32)
+        out = (C.c_double * 6)()
+        A.check(A.lib().axon_profile_present(self._h, A.u32(stim), T, clamp_steps, int(learn), use_bias, out))
+        return {"drive_us": out[0], "barrier_us": out[1], "emit_us": out[2], "learn_us": out[3], "step_us": out[4],
+                "launch_ms": out[5]}
+
     def set_wait_limit(self, ns: int) -> None:
         A.check(A.lib().axon_set_wait_limit(self._h, ns))
 

@@ -318,6 +318,21 @@ axon_status axon_serve_wait_idle(axon_server* s, double timeout_s);
 axon_status axon_serve_stats(axon_server* s, axon_serve_counters* out);
 axon_status axon_serve_destroy(axon_server* s);
 
+/* A second network with the same configuration and a copy of every device buffer of
+ * `src` (planes, conn, bias, mult, the per-present buffers). No counterpart in the
+ * reference; the profile mode uses it so that profiling changes no network. */
+axon_status axon_clone(const axon_net* src, axon_net** out);
+
+/* profile=1 of the reference (src/axon.mm:1161-1256) times each of its five kernels with
+ * Metal timestamps over one learning presentation. Here the five run fused in one
+ * persistent launch, so the same presentation is timed per phase with the device timer:
+ * out[0..3] = us per step of drive + k-of-32 (k_drive, the ballot of k_emit), the grid
+ * barrier, threshold + gate + spike rebuild (k_topk, k_emit), records + bias + learning
+ * (k_emit's counters, k_bias, k_learn), each the mean over CTAs; out[4] = us per step;
+ * out[5] = the launch in ms. The presentation itself is an ordinary axon_present. */
+axon_status axon_profile_present(axon_net* net, const uint32_t* stim, uint32_t T, uint32_t clamp_steps, int learn,
+                                 uint32_t use_bias, double out[6]);
+
 /* Grid-wait limit of the persistent kernels in nanoseconds (default 2e9). */
 axon_status axon_set_wait_limit(axon_net* net, uint64_t ns);
 /* No counterpart in the reference (it has no failure detection). Test hook for the bounded

@@ -67,3 +67,20 @@ def test_cli_spot_check_full_size():
         g["within_pct"], g["recall"], g["best_other"], g["sustained"], g["drive_t6"])
     ref = comparable(O.run_cli(args))
     assert comparable(out) == ref
+
+
+def test_profile_mode_times_phases_and_changes_nothing_else():
+    """profile=1 (the reference's per-kernel GPU profile, src/axon.mm:1161-1256) prints the
+    per-phase device-timer profile of one learning presentation; it runs on a copy of the
+    network, so every other line equals the run without it."""
+    base = [*SMALL, *CONFIG_C, "stim=3", "epochs=1", "deep=1"]
+    plain = comparable(engine_cli(base))
+    out = engine_cli([*base, "profile=1"]).splitlines()
+    i = next(k for k, ln in enumerate(out) if "PER-PHASE GPU PROFILE" in ln)
+    j = next(k for k in range(i + 1, len(out)) if out[k].startswith("====="))
+    rows = {ln[:42].strip(): ln[42:].split() for ln in out[i + 3:j - 3]}
+    total = float(out[j - 3][42:].split()[0])
+    parts = [float(v[0]) for v in rows.values()]
+    assert len(parts) == 4 and all(p >= 0 for p in parts) and abs(sum(parts) - total) <= 0.05 * total + 0.5
+    rest = out[:i - 1] + out[j + 1:]  # the profile block and the blank line before it
+    assert comparable("\n".join(rest)) == plain
