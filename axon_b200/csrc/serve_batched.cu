@@ -184,16 +184,22 @@ __global__ void __launch_bounds__(1024, 1) k_serve_batched(ServeDev d, ServeCfg 
     __syncthreads();
     // per-neuron and column drives of the item's columns into every trajectory's slot
     const uint32_t accOff = serve_acc_off(ncol), xOff = 2u * ncol + 2u * d.nactw;
-    if (PACK) {  // the packed counters are the u16 drives: half a warp per (column, trajectory)
-      const uint32_t half = lane >> 4, l16 = lane & 15u;
-      for (uint32_t pp = warp * 2u + half; pp < kRecallCpi * B; pp += nw * 2u) {
+    if (PACK) {  // the packed counters are the u16 drives: four lanes per (column, trajectory),
+                 // each storing 4 of its 16 words as one 16-byte vector
+      const uint32_t q = lane & 3u, grp = lane >> 2;
+      const uint32_t gmask = 0xFu << (grp * 4u);
+      for (uint32_t pp = warp * 8u + grp; pp < kRecallCpi * B; pp += nw * 8u) {
         const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
-        if (col >= ncol) continue;  // uniform over the half warp
+        if (col >= ncol) continue;  // uniform over the four lanes
         uint32_t* base = d.slots + (size_t)__ldg(d.btab + bn.tabOff + b).x * d.slotWords;
-        const uint32_t w = sAcc[(colL * B + b) * accStride + l16];
-        __stcg(base + accOff + col * 16u + l16, w);
-        const uint32_t dsum = __reduce_add_sync(half ? 0xFFFF0000u : 0x0000FFFFu, (w & 0xFFFFu) + (w >> 16));
-        if (l16 == 0) __stcg(base + xOff + col, dsum);
+        const uint32_t* src = sAcc + (colL * B + b) * accStride + q * 4u;
+        const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
+        __stcg(reinterpret_cast<uint4*>(base + accOff + col * 16u) + q, w);
+        uint32_t s = (w.x & 0xFFFFu) + (w.x >> 16) + (w.y & 0xFFFFu) + (w.y >> 16) + (w.z & 0xFFFFu) + (w.z >> 16) +
+                     (w.w & 0xFFFFu) + (w.w >> 16);
+        s += __shfl_xor_sync(gmask, s, 1);
+        s += __shfl_xor_sync(gmask, s, 2);
+        if (q == 0) __stcg(base + xOff + col, s);
       }
     } else {
       for (uint32_t pp = warp; pp < kRecallCpi * B; pp += nw) {
