@@ -66,20 +66,28 @@ __global__ void __launch_bounds__(1024, 1) k_serve_batched(ServeDev d, ServeCfg 
     return d.slots + (size_t)st.x * d.slotWords + ((st.y - 1u) & 1u) * ncol;
   };
 
+  // thread 0 claims one item ahead: the claim's round trip overlaps the current item
+  uint32_t claim = nitems;
   if (tid == 0) {
     const uint32_t it0 = atomicAdd(d.work, 1u);
     sMisc[1] = it0;
-    if (it0 < nitems) issue(it0, kbuf);
+    if (it0 < nitems) {
+      issue(it0, kbuf);
+      claim = atomicAdd(d.work, 1u);
+    }
   }
   __syncthreads();
   uint32_t item = sMisc[1];
   while (item < nitems) {
     const uint32_t bcur = kbuf;
     if (tid == 0) {
-      const uint32_t nx = atomicAdd(d.work, 1u);
+      const uint32_t nx = claim;
       sMisc[2] = nx;
       sMisc[3] = 0u;
-      if (nx < nitems) issue(nx, bcur ^ 1u);
+      if (nx < nitems) {
+        issue(nx, bcur ^ 1u);
+        claim = atomicAdd(d.work, 1u);
+      }
     }
     const ServeBNet bn = d.bnets[item / nip];
     const uint32_t* conn = d.nets[bn.net].conn;
