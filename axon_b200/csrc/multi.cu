@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(NT, 1) k_multi(MultiDev m, MultiCfg c) {
         {
           const uint4* W3 = sNet.d.W3;
           const uint32_t* conn = sNet.d.conn;
-          const uint32_t* biasG = sNet.d.bias;
+          uint32_t* biasG = sNet.d.bias;
           uint32_t* accG = sNet.d.acc;
           uint32_t* bbG = sNet.d.bbits;
           uint32_t* xdrive = sNet.d.xdrive + par * ncol;
@@ -142,7 +142,16 @@ __global__ void __launch_bounds__(NT, 1) k_multi(MultiDev m, MultiCfg c) {
             if (cc >= ncol) break;  // warp-uniform
             const uint32_t cn = cnNext;
             if (cc + nwS < ncol) cnNext = __ldg(conn + (cc + nwS) * kNslot + lane);
-            const uint32_t bsrc = useBias ? __ldcg(biasG + cc * 32u + lane) : 0u;
+            // k_bias of the previous step (src/axon.mm:240-253) runs here, on the bias value
+            // this step's drive reads anyway: fired(t-1) is the bit of spk(t-1)
+            const bool biasStep = learn && t > 0u && cc >= incols;
+            uint32_t bsrc = (useBias || biasStep) ? __ldcg(biasG + cc * 32u + lane) : 0u;
+            if (biasStep) {
+              const int dec = (((t - 1u) % max(c.biasDownEvery, 1u)) == 0u) ? (int)c.biasDown : 0;
+              const int nbv = (int)bsrc + (((sIn[cc] >> lane) & 1u) ? (int)c.biasUp : -dec);
+              bsrc = (uint32_t)max(0, nbv);
+              __stcg(biasG + cc * 32u + lane, bsrc);
+            }
             uint32_t active = __ballot_sync(kFull, (sActIn[cn >> 5] >> (cn & 31u)) & 1u);
             nTiles += __popc(active);
             uint32_t a = 0, b2 = 0;
@@ -262,12 +271,7 @@ __global__ void __launch_bounds__(NT, 1) k_multi(MultiDev m, MultiCfg c) {
               }
             }
             if (!learn) continue;
-            // k_bias, src/axon.mm:240-253
-            if (recur) {
-              const int dec = ((t % max(c.biasDownEvery, 1u)) == 0u) ? (int)c.biasDown : 0;
-              const int nbv = (int)__ldcg(biasG + cc * 32u + lane) + (fired ? (int)c.biasUp : -dec);
-              __stcg(biasG + cc * 32u + lane, (uint32_t)max(0, nbv));
-            }
+            // (k_bias of this step runs in the next step's phase A, or after the last step)
             // k_learn, src/axon.mm:436-495: the column learns this step
             if (phase == 3u || b == 0u) continue;
             if (c.marginGate != 0u && !(vk > vk1)) continue;
@@ -355,7 +359,29 @@ __global__ void __launch_bounds__(NT, 1) k_multi(MultiDev m, MultiCfg c) {
         __syncthreads();  // sOut / sActOut complete before the next step reads them
       }
 
-      // ---------------- end of the presentation: the buffers present() leaves behind
+      // ---------------- end of the presentation: k_bias of the last step, then the buffers
+      // present() leaves behind
+      if (learn) {
+        const uint32_t* sLast = (T & 1u) ? sSpk1 : sSpk0;  // spk(T-1)
+        const int dec = (((T - 1u) % max(c.biasDownEvery, 1u)) == 0u) ? (int)c.biasDown : 0;
+        uint32_t* biasG = sNet.d.bias;
+        const uint32_t first = gw + ((incols > gw) ? ((incols - gw + nwS - 1u) / nwS) * nwS : 0u);  // first owned recurrent column
+        for (uint32_t c0 = first; c0 < ncol; c0 += 4u * nwS) {  // four columns' loads in flight
+          uint32_t v[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const uint32_t cc = c0 + (uint32_t)k * nwS;
+            v[k] = cc < ncol ? __ldcg(biasG + cc * 32u + lane) : 0u;
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const uint32_t cc = c0 + (uint32_t)k * nwS;
+            if (cc >= ncol) break;
+            const int nbv = (int)v[k] + (((sLast[cc] >> lane) & 1u) ? (int)c.biasUp : -dec);
+            __stcg(biasG + cc * 32u + lane, (uint32_t)max(0, nbv));
+          }
+        }
+      }
       {
         const uint32_t* sLast = (T & 1u) ? sSpk1 : sSpk0;  // spk(T-1)
         const uint32_t* sPrev = (T & 1u) ? sSpk0 : sSpk1;  // spk(T-2), zero when T == 1
