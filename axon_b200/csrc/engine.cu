@@ -18,7 +18,9 @@ namespace axon {
 // Configurations the kernels are built for. The reference accepts some of these and then
 // indexes past its fixed buffers or divides by zero; here they are refused.
 std::string validate_cfg(const axon_cfg& c) {
-  if (c.ncol == 0 || c.ncol % 32 != 0 || c.ncol > 16384) return "ncol must be a multiple of 32 in [32, 16384]";
+  // the fused step keeps two spike vectors, the drives and the ballots of the whole
+  // network in each CTA's shared memory: 8,192 columns is the widest that fits every kernel
+  if (c.ncol == 0 || c.ncol % 32 != 0 || c.ncol > 8192) return "ncol must be a multiple of 32 in [32, 8192]";
   if (c.incols >= c.ncol) return "incols must be below ncol";
   if (c.inbr > 32) return "inbr must be <= 32";
   const uint32_t nInGrp = c.incols / 8, nGrp = c.ncol / 8;
@@ -85,12 +87,12 @@ axon_status axon_net::create(const axon_cfg& c, int dev) {
   CK(cudaMallocHost(&hstim, (size_t)ncol * 4));
   CK(cudaMallocHost(&hscratch, 64 * 4));
 
-  // launch shape: one column per warp when the grid fits in one wave, else 2 or 4
+  // launch shape: one column per warp when the grid fits in one wave, else 2
   cudaDeviceProp prop;
   CK(cudaGetDeviceProperties(&prop, device));
   sm_count = prop.multiProcessorCount;
   bool ok = false;
-  for (int cpw : {1, 2, 4}) {
+  for (int cpw : {1, 2}) {
     const uint32_t warps = (ncol + cpw - 1) / cpw;
     int wpb = (int)std::min<uint32_t>(32, (warps + prop.multiProcessorCount - 1) / prop.multiProcessorCount);
     wpb = std::max(wpb, 1);

@@ -317,7 +317,6 @@ cudaError_t launch_present(const NetDev& d, const PresentCfg& c, const LaunchSha
   switch (ls.cpw) {
     case 1: fn = (const void*)k_present<1>; break;
     case 2: fn = (const void*)k_present<2>; break;
-    case 4: fn = (const void*)k_present<4>; break;
     default: return cudaErrorInvalidValue;
   }
   return cudaLaunchCooperativeKernel(fn, dim3(ls.grid), dim3(ls.wpb * 32), args, ls.smem, st);
@@ -328,7 +327,6 @@ cudaError_t present_max_blocks_per_sm(int cpw, int threads, size_t smem, int* ou
   switch (cpw) {
     case 1: fn = (const void*)k_present<1>; break;
     case 2: fn = (const void*)k_present<2>; break;
-    case 4: fn = (const void*)k_present<4>; break;
     default: return cudaErrorInvalidValue;
   }
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -27,7 +27,7 @@ struct PresentCfg {
 };
 
 struct LaunchShape {
-  int cpw;       // columns per warp (1, 2, 4)
+  int cpw;       // columns per warp (1, 2)
   int wpb;       // warps per block
   int grid;      // blocks (all co-resident)
   size_t smem;   // dynamic shared memory bytes

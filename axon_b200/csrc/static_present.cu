@@ -110,7 +110,7 @@ extern "C" axon_status axon_present_static(const axon_cfg* cfg, const axon_state
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   LaunchShape ls{};
   bool ok = false;
-  for (int cpw : {1, 2, 4}) {
+  for (int cpw : {1, 2}) {
     const uint32_t warps = (ncol + cpw - 1) / cpw;
     int wpb = (int)((warps + sms - 1) / sms);
     wpb = wpb < 1 ? 1 : (wpb > 32 ? 32 : wpb);

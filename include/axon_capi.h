@@ -34,7 +34,7 @@ typedef enum axon_status {
  * src/axon.mm:688-735 (key name in brackets). `bandhi` is the key value: the engine
  * applies it only when `contrast` != 0, as src/axon.mm:812 does. */
 typedef struct axon_cfg {
-  uint32_t ncol;          /* [ncol] columns of 32 neurons, multiple of 32, <= 16384 */
+  uint32_t ncol;          /* [ncol] columns of 32 neurons, multiple of 32, <= 8192 */
   uint32_t incols;        /* [incols] clamped input columns */
   uint32_t inbr;          /* [inbr] afferent branches of 32 */
   uint32_t nand;          /* [nand] initial functional density 2^-nand */

@@ -152,3 +152,55 @@ def test_diagnostics_match_oracle():
     asm = np.stack([ball, np.roll(ball, 8), np.roll(ball, 16)]).astype(np.uint32)
     for sel in (0, 1, 2):
         assert np.array_equal(gpu.wdiag(memb, asm, 3, sel), cpu.wdiag(memb, asm, 3, sel))
+
+
+@pytest.mark.parametrize("ncol", [8192])
+def test_widest_network_two_columns_per_warp(ncol):
+    """ncol 8,192, the widest network the engine takes, runs k_present with 2 columns per
+    warp (the grid must fit one wave of co-resident CTAs): learning and readout
+    presentations against the oracle; a wider network is refused at creation."""
+    import axon_b200 as ax
+
+    with pytest.raises(ax._capi.AxonError):
+        ax.Network(make_cfg(ncol=16384, incols=512))
+
+    cfg = make_cfg(ncol=ncol, incols=512, target=64, k=24)
+    gpu = ax.Network(cfg)
+    cpu = O.OracleNet(cfg)
+    gpu.init(5)
+    cpu.init(5)
+    pats = ax.stimuli(5, 2, cfg.incols, 64)
+    for p in range(2):
+        stim = ax.load_stim(pats[p], 1.0, 1000 + p, cfg.ncol)
+        gpu.present(stim, 8, 4, True)
+        cpu.present(stim, 8, 4, True)
+        compare(gpu, cpu, BUFS_EACH_PRESENT + ["HIST"], T=8, where=f"ncol {ncol} learn p{p}")
+    planes_equal(gpu, cpu, f"ncol {ncol}")
+    stim = ax.load_stim(pats[1], 0.75, 4401, cfg.ncol)
+    gpu.present(stim, 12, 4, False, True, 0)
+    cpu.present(stim, 12, 4, False, True, 0)
+    compare(gpu, cpu, BUFS_EACH_PRESENT + ["HIST"], T=12, where=f"ncol {ncol} readout")
+    gpu.close()
+    cpu.close()
+
+
+@pytest.mark.parametrize("T,clamp", [(1, 0), (1, 1), (64, 0), (64, 64), (3, 2)])
+def test_step_count_limits(T, clamp):
+    """The shortest and longest presentations (T = 1 and T = 64, the hist capacity), with
+    no clamped step and with every step clamped."""
+    import axon_b200 as ax
+
+    cfg = make_cfg()
+    gpu = ax.Network(cfg)
+    cpu = O.OracleNet(cfg)
+    gpu.init(2)
+    cpu.init(2)
+    pats = ax.stimuli(2, 2, cfg.incols, 16)
+    for learn in (True, False):
+        stim = ax.load_stim(pats[0], 1.0, 1000, cfg.ncol)
+        gpu.present(stim, T, clamp, learn)
+        cpu.present(stim, T, clamp, learn)
+        compare(gpu, cpu, BUFS_EACH_PRESENT + ["HIST"], T=T, where=f"T{T} clamp{clamp} learn{learn}")
+    planes_equal(gpu, cpu, f"T{T}")
+    gpu.close()
+    cpu.close()

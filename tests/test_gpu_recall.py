@@ -96,3 +96,21 @@ def test_recall_batched_equals_plain_full_geometry():
     f, h, _, _ = oracle_runs(cpu, cues[idx], 45, 10, 0)
     assert np.array_equal(rb["final"][idx], f)
     assert np.array_equal(rb["hist"][idx], h)
+
+
+def test_batched_equals_plain_at_the_widest_batched_network():
+    """ncol = 8,192, the widest network the batched kernel takes (the plain path at that
+    width is checked against the oracle in test_gpu_plain): both methods agree on every
+    trajectory's spikes at every step."""
+    import axon_b200 as ax
+
+    cfg = ax.config(ncol=8192, incols=512, **ax.CONFIG_C)
+    with ax.Network(cfg) as net:
+        net.init(4)
+        pats = ax.stimuli(4, 6, 512, 64)
+        for p in range(6):
+            net.present(ax.load_stim(pats[p], 1.0, 1000 + p, 8192), 10, 5, True)
+        cues = np.stack([ax.load_stim(pats[q % 6], 0.6 + 0.05 * (q % 5), 4400 + q, 8192) for q in range(20)])
+        a = net.recall(cues, 25, 6, hist=True)
+        b = net.recall(cues, 25, 6, hist=True, method="plain")
+        assert np.array_equal(a["hist"], b["hist"]) and np.array_equal(a["final"], b["final"])
