@@ -121,6 +121,11 @@ __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
   return *reinterpret_cast<const volatile uint32_t*>(p);
 }
+// arrival at a grid barrier: a release at GPU scope (cumulative over the writes the CTA's
+// threads made before the preceding __syncthreads) that does not wait for a reply
+__device__ __forceinline__ void red_release_add_gpu(uint32_t* p, uint32_t v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 // Grid-wide barrier over `nblocks` co-resident CTAs. `bar` is zeroed before the launch;
 // barrier number `epoch` (0, 1, 2, ...) waits until all CTAs have arrived `epoch+1`
@@ -132,8 +137,7 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t* err, uint3
   __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t ok = 1;
-    __threadfence();
-    atomicAdd(bar, 1u);
+    red_release_add_gpu(bar, 1u);
     const uint32_t target = (epoch + 1u) * nblocks;
     const uint64_t t0 = globaltimer_ns();
     uint32_t it = 0;
@@ -146,8 +150,7 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t* err, uint3
         }
       }
     }
-    __threadfence();
-    *s_flag = ok;
+    *s_flag = ok;  // the acquire load that saw the count orders the CTA's later reads
   }
   __syncthreads();
   return *s_flag != 0u;
