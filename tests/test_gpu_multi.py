@@ -93,3 +93,28 @@ def test_training_only_and_bad_arguments():
     finally:
         for n in nets:
             n.close()
+
+
+@pytest.mark.parametrize("variant", [dict(margingate=1, hetero=1, ltdrep=2, ltdevery=1), dict(contrast=0),
+                                     dict(mode=0, dthr=2), dict(mode=2, dthr=3, boost=7), dict(topkpar=0),
+                                     dict(biasdownevery=3, biasshift=2, ktest=8, facil=5)])
+def test_rule_variants_one_launch_equals_plain(variant):
+    """Learning-rule and mode variants: the one-launch form leaves the same weights, bias
+    and measurements as the plain path."""
+    cfg = dict(SMALL_CFG, **variant)
+
+    def run(method, **kw):
+        nets = [ax.Network(cfg) for _ in range(3)]
+        try:
+            res, _ = ax.multi_train(nets, [0, 1, 2], [3, 4, 2], epochs=2, stimcols=16, method=method, **kw)
+            return res, [{b: n.read(b) for b in PLANES} for n in nets]
+        finally:
+            for n in nets:
+                n.close()
+
+    a = run("launch", autotune=False, slots=3, threads=512, graph=False)
+    b = run("plain")
+    assert a[0] == b[0]
+    for x, y in zip(a[1], b[1]):
+        for name in PLANES:
+            assert np.array_equal(x[name], y[name]), (variant, name)

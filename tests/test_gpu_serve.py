@@ -105,3 +105,24 @@ def test_bad_requests(fleet):
             srv.submit(0, [1], 0, 0, 0)  # no steps
     with pytest.raises(ax._capi.AxonError):
         ax.Server(nets, 1024)  # budget below one slot
+
+
+@pytest.mark.parametrize("variant", [dict(facil=40, ktest=5), dict(boost=2000), dict(mode=2, dthr=2, boost=0),
+                                     dict(mode=0, dthr=3)])
+def test_variants_in_the_mix_equal_recall(variant):
+    """Readout variants through both drive kernels: facilitation (u32 counters in the
+    batched kernel), drives past 16 bits (u32 slabs), the two-layer and point modes. Each
+    request's final spikes equal axon_recall's for that network and cue."""
+    cfg = dict(CFG, **variant)
+    nets = [ax.Network(cfg) for _ in SEEDS]
+    try:
+        ax.multi_train(nets, SEEDS, LOADS, epochs=1, stimcols=STIMCOLS, readout=False, autotune=False, slots=3)
+        pats = [ax.stimuli(s, L, 64, STIMCOLS) for s, L in zip(SEEDS, LOADS)]
+        reqs = requests(pats, 110, 7)  # about 37 per network: the batched drive runs
+        mix, st = serve(nets, reqs)
+        assert st["max_batch"] > 3 * 24
+        for r in reqs:
+            assert np.array_equal(mix[r["tag"]][1], alone_by_recall(nets, r)), (variant, r["tag"])
+    finally:
+        for n in nets:
+            n.close()
