@@ -33,7 +33,7 @@ class AxonCfg(C.Structure):
 
 class RecallArgs(C.Structure):
     _fields_ = [("T", C.c_uint32), ("clamp_steps", C.c_uint32), ("use_bias", C.c_uint32), ("method", C.c_uint32),
-                ("reserved", C.c_uint32 * 4)]
+                ("graph", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 RECALL_BATCHED, RECALL_PLAIN = 0, 1

@@ -114,6 +114,8 @@ axon_status axon_net::create(const axon_cfg& c, int dev) {
 }
 
 void axon_net::release() {
+  if (recallGraph) cudaGraphExecDestroy(recallGraph);
+  recallGraph = nullptr;
   scratch.release();
   io.release();
   if (w3b) cudaFree(w3b);

@@ -4,6 +4,7 @@
 #pragma once
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -75,4 +76,7 @@ struct axon_net {
   axon_status recall(const uint32_t* cues, uint32_t B, const axon_recall_args& a, const uint32_t* refBall,
                      uint32_t* finalOut, uint32_t* hist, uint32_t* stats, uint32_t* driveLog, bool dev, double* ms);
   axon_status ensure_w3b();
+  // the batched readout as a captured CUDA graph, with the arguments it was captured for
+  cudaGraphExec_t recallGraph = nullptr;
+  std::vector<uint64_t> recallKey;
 };

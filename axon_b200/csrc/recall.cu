@@ -163,8 +163,21 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     CK(recall_max_blocks_per_sm(rc.acc32, rs.threads, rs.smem, &per_sm));
     if (per_sm < 1) return set_error(AXON_EINVAL, "batched recall kernel does not fit one SM");
     rs.grid = sm_count * per_sm;
-    CK(cudaEventRecord(ev0, stream));
-    for (uint32_t b0 = 0; b0 < B; b0 += Bc) {  // one launch per chunk of trajectories
+    // everything the launches depend on: a captured graph is replayed only for the same key
+    const std::vector<uint64_t> key = {(uint64_t)dCues, (uint64_t)dRef, (uint64_t)dFinal, (uint64_t)dHist,
+                                       (uint64_t)dStats, (uint64_t)dLog, (uint64_t)scratch.p, (uint64_t)w3b, B, a.T,
+                                       a.clamp_steps, a.use_bias, (uint64_t)rs.grid, wait_ns};
+    const bool graph = a.graph != 0u;
+    const bool replay = graph && recallGraph && key == recallKey;
+    if (graph && !replay) {
+      if (recallGraph) cudaGraphExecDestroy(recallGraph);
+      recallGraph = nullptr;
+      recallKey.clear();
+      CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    }
+    if (!graph) CK(cudaEventRecord(ev0, stream));
+    cudaError_t e = cudaSuccess;  // a failure inside a capture still ends the capture
+    for (uint32_t b0 = 0; replay == false && b0 < B; b0 += Bc) {  // one launch per chunk of trajectories
       const uint32_t nb = std::min(Bc, B - b0);
       rc.B = nb;
       rd.stims = dCues + (size_t)b0 * ncol;
@@ -173,12 +186,30 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
       rd.hist = dHist ? dHist + (size_t)b0 * a.T * ncol : nullptr;
       rd.stats = dStats ? dStats + (size_t)b0 * 1024 : nullptr;
       rd.driveLog = dLog ? dLog + (size_t)b0 * 256 : nullptr;
-      CK(cudaMemsetAsync(rd.spk, 0, (size_t)nb * ncol * 4, stream));
-      CK(cudaMemsetAsync(rd.ecnt, 0, 2ull * ngrp * 4, stream));
-      CK(cudaMemsetAsync(rd.work, 0, 64 * 4, stream));
-      CK(cudaMemsetAsync(rd.thPrev, 0, (size_t)nb * 4, stream));
-      CK(cudaMemsetAsync(d.bar, 0, 4, stream));
-      CK(launch_recall(rd, rc, rs, stream));
+      if (e == cudaSuccess) e = cudaMemsetAsync(rd.spk, 0, (size_t)nb * ncol * 4, stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(rd.ecnt, 0, 2ull * ngrp * 4, stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(rd.work, 0, 64 * 4, stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(rd.thPrev, 0, (size_t)nb * 4, stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(d.bar, 0, 4, stream);
+      if (e == cudaSuccess) e = launch_recall(rd, rc, rs, stream);
+      if (e != cudaSuccess) break;
+    }
+    if (graph && !replay) {
+      cudaGraph_t g = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(stream, &g);
+      if (e == cudaSuccess) e = ec;
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&recallGraph, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        recallGraph = nullptr;
+        return cuda_fail(e, "batched recall graph capture");
+      }
+      recallKey = key;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "launch_recall");
+    if (graph) {
+      CK(cudaEventRecord(ev0, stream));
+      CK(cudaGraphLaunch(recallGraph, stream));
     }
     CK(cudaEventRecord(ev1, stream));
   }

@@ -117,7 +117,7 @@ class Network:
 
     def recall(self, cues: np.ndarray, T: int, clamp_steps: int, use_bias: int = 0, method: str = "batched",
                hist: bool = False, stats: bool = False, ref_ball: np.ndarray | None = None,
-               drive_log: np.ndarray | None = None) -> dict:
+               drive_log: np.ndarray | None = None, graph: bool = False) -> dict:
         """B readout trajectories (present() with learn=0 for each cue row) in one call.
 
         Returns {"final": (B, ncol), "hist": (B, T, ncol) | None, "stats": (B, 1024) | None,
@@ -127,7 +127,7 @@ class Network:
         B = cues.shape[0]
         assert cues.shape == (B, self.ncol)
         a = A.RecallArgs(T=T, clamp_steps=clamp_steps, use_bias=use_bias,
-                         method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN)
+                         method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN, graph=int(graph))
         out = {"final": np.empty((B, self.ncol), dtype=np.uint32),
                "hist": np.empty((B, T, self.ncol), dtype=np.uint32) if hist else None,
                "stats": np.empty((B, 1024), dtype=np.uint32) if stats else None,
@@ -147,10 +147,11 @@ class Network:
         return out
 
     def recall_device(self, cues_ptr: int, B: int, T: int, clamp_steps: int, final_ptr: int | None = None,
-                      use_bias: int = 0, method: str = "batched") -> float:
-        """Device-resident variant: cues/final are device addresses on this network's GPU."""
+                      use_bias: int = 0, method: str = "batched", graph: bool = False) -> float:
+        """Device-resident variant: cues/final are device addresses on this network's GPU.
+        graph=True replays a captured CUDA graph of the launch while the arguments repeat."""
         a = A.RecallArgs(T=T, clamp_steps=clamp_steps, use_bias=use_bias,
-                         method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN)
+                         method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN, graph=int(graph))
         ms = C.c_double()
         A.check(A.lib().axon_recall_device(self._h, C.c_void_p(cues_ptr), B, C.byref(a), None,
                                            None if final_ptr is None else C.c_void_p(final_ptr), None, None, None,

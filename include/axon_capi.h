@@ -156,7 +156,10 @@ typedef struct axon_recall_args {
   uint32_t clamp_steps; /* leading steps clamped to the cue */
   uint32_t use_bias;    /* 0 off (the reference's readout default), 1 on */
   uint32_t method;      /* axon_recall_method */
-  uint32_t reserved[4]; /* zero */
+  uint32_t graph;       /* batched method: 1 = run the launch(es) and their buffer resets as a
+                           captured CUDA graph, kept and replayed while every argument and
+                           array stays the same (device-resident callers); 0 = launch directly */
+  uint32_t reserved[3]; /* zero */
 } axon_recall_args;
 
 axon_status axon_recall(axon_net* net, const uint32_t* cues, uint32_t B, const axon_recall_args* args,

@@ -114,3 +114,22 @@ def test_batched_equals_plain_at_the_widest_batched_network():
         a = net.recall(cues, 25, 6, hist=True)
         b = net.recall(cues, 25, 6, hist=True, method="plain")
         assert np.array_equal(a["hist"], b["hist"]) and np.array_equal(a["final"], b["final"])
+
+
+def test_graph_replay_equals_direct_launch():
+    """graph=1 captures the batched launch once and replays it while the arguments repeat;
+    the results equal a direct launch, also after the weights change (the tile layout is
+    rebuilt in place, so the replayed graph reads the new weights)."""
+    import axon_b200 as ax
+
+    cfg, gpu, cpu, pats = trained_pair({}, 4, 1, 16)
+    cues = make_cues(pats, cfg.ncol, 12, np.random.default_rng(3))
+    direct = gpu.recall(cues, 20, 5, hist=True)
+    g1 = gpu.recall(cues, 20, 5, hist=True, graph=True)  # captured
+    g2 = gpu.recall(cues, 20, 5, hist=True, graph=True)  # replayed
+    for r in (g1, g2):
+        assert np.array_equal(r["hist"], direct["hist"]) and np.array_equal(r["final"], direct["final"])
+    gpu.present(ax.load_stim(pats[0], 1.0, 1000, cfg.ncol), 10, 5, True)
+    after = gpu.recall(cues, 20, 5, hist=True)
+    g3 = gpu.recall(cues, 20, 5, hist=True, graph=True)
+    assert np.array_equal(g3["hist"], after["hist"])
