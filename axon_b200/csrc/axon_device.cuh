@@ -85,16 +85,30 @@ __device__ __forceinline__ void bs_clip(uint32_t& a0, uint32_t& a1, uint32_t& a2
 // ---------------------------------------------------------------- exact k-of-32
 // rank = #{j : v_j > v_i or (v_j == v_i and j < i)}; winners rank < k; vk / vk1 are the
 // values ranked k-1 and k (0 if no lane has that rank). src/axon.mm:134-144.
+// Method: the value ranked k-1 by a most-significant-bit-first radix select over the bits of
+// the largest value, with the lanes that still match the selected prefix kept as a ballot
+// mask (every step is warp-uniform); then every lane above it wins, and of the lanes equal
+// to it the lowest ones fill the remaining places.
 __device__ __forceinline__ uint32_t warp_kwta(uint32_t v, uint32_t lane, uint32_t k, uint32_t& vk, uint32_t& vk1) {
-  uint32_t rank = 0;
-#pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    const uint32_t ov = __shfl_sync(kFull, v, j);
-    rank += (ov > v || (ov == v && (uint32_t)j < lane)) ? 1u : 0u;
+  (void)lane;
+  if (k == 0u) { vk = 0u; vk1 = __reduce_max_sync(kFull, v); return 0u; }
+  if (k > 32u) { vk = 0u; vk1 = 0u; return kFull; }
+  const uint32_t M = __reduce_max_sync(kFull, v);
+  uint32_t m = kFull, prefix = 0u, rem = k;
+  for (int bit = (int)(32u - __clz(M)) - 1; bit >= 0; --bit) {
+    const uint32_t ones = m & __ballot_sync(kFull, (v >> bit) & 1u);
+    const uint32_t c1 = (uint32_t)__popc(ones);
+    if (c1 >= rem) { m = ones; prefix |= 1u << bit; } else { rem -= c1; m &= ~ones; }
   }
-  vk = __reduce_max_sync(kFull, rank == k - 1u ? v : 0u);
-  vk1 = __reduce_max_sync(kFull, rank == k ? v : 0u);
-  return __ballot_sync(kFull, rank < k);
+  vk = prefix;
+  const uint32_t gt = __ballot_sync(kFull, v > prefix), eq = __ballot_sync(kFull, v == prefix);
+  const uint32_t ngt = (uint32_t)__popc(gt), need = k - ngt;  // 1 <= need <= popc(eq)
+  const uint32_t pos = __fns(eq, 0u, (int)need);               // the need-th lowest lane equal to vk
+  const uint32_t low = eq & ((2u << pos) - 1u);
+  if (k == 32u) vk1 = 0u;
+  else if (ngt + (uint32_t)__popc(eq) > k) vk1 = prefix;
+  else vk1 = __reduce_max_sync(kFull, v < prefix ? v : 0u);
+  return gt | low;
 }
 
 // ---------------------------------------------------------------- asynchronous copies

@@ -45,7 +45,7 @@ axon_status axon_net::create(const axon_cfg& c, int dev) {
   CK(cudaEventCreate(&ev1));
   // one allocation: 4 planes, then the small buffers, each 256-byte aligned
   const uint64_t small[] = {(uint64_t)ncol * 32, ncol, ncol, ncol, n, n, n, ncol, ncol, 256, n, ncol, 1024,
-                            64ull * ncol, 16, 2ull * ncol, 2ull * ncol, 64, 64};
+                            64ull * ncol, 16, 2ull * ncol, 2ull * ncol, kBarRegionWords, 64};
   uint64_t total = 4 * plane_words * 4;
   for (uint64_t w : small) total += (w * 4 + 255) & ~255ull;
   base_bytes = total;
@@ -195,7 +195,6 @@ axon_status axon_net::present(const uint32_t* stim, uint32_t T, uint32_t clampSt
   std::memcpy(hstim, stim, (size_t)ncol * 4);
   CK(cudaMemcpyAsync(d.stim, hstim, (size_t)ncol * 4, cudaMemcpyHostToDevice, stream));
   CK(cudaMemsetAsync(d.stats, 0, 1024 * 4, stream));
-  CK(cudaMemsetAsync(d.bar, 0, 4, stream));
   PresentCfg pc = present_cfg(T, clampSteps, learn, useBias);
   pc.missing = inject_missing;
   inject_missing = 0;
@@ -352,7 +351,6 @@ axon_status axon_net::profile_present(const uint32_t* stim, uint32_t T, uint32_t
   std::memcpy(hstim, stim, (size_t)ncol * 4);
   CK(cudaMemcpyAsync(d.stim, hstim, (size_t)ncol * 4, cudaMemcpyHostToDevice, stream));
   CK(cudaMemsetAsync(d.stats, 0, 1024 * 4, stream));
-  CK(cudaMemsetAsync(d.bar, 0, 4, stream));
   CK(cudaMemsetAsync(tmp.p, 0, nst * 8, stream));
   NetDev dd = d;
   dd.prof = (unsigned long long*)tmp.p;

@@ -373,7 +373,6 @@ axon_status MultiRun::run_plain(float* ms) {
       dd.driveLog = p.driveLog ? p.driveLog : sDlog;
       dd.finalOut = p.finalOut;
       const PresentCfg pc = net->present_cfg(p.T, p.clampSteps, p.learn != 0u, p.useBias);
-      CK(cudaMemsetAsync(net->d.bar, 0, 4, st));
       CK(launch_present(dd, pc, net->shape, st));
     }
   }

@@ -5,8 +5,12 @@
 // the whole step loop is one cooperative launch with ONE grid barrier per step:
 //
 //   phase A  each warp owns one column (lane = neuron): drive over the column's non-silent
-//            branches (W3 tiles streamed from HBM, spikes from shared memory), the exact
-//            k-of-32 ballot, and the column drive; drive + ungated ballot are published.
+//            branches, the exact k-of-32 ballot, and the column drive; drive + ungated
+//            ballot are published, and the drive is counted into the step's histogram.
+//            The W3 tiles of the non-silent branches of all the CTA's columns are in flight
+//            at once: each branch's lane issues one 1 KiB TMA bulk copy into a CTA-wide
+//            shared-memory pool (slots claimed per column), completed on a per-column
+//            mbarrier; spikes come from shared memory.
 //   barrier
 //   phase B  every CTA reads all published drives/ballots (L2), selects the column
 //            threshold (the target-th largest recurrent drive) and rebuilds the whole
@@ -20,6 +24,7 @@
 #include <cstdint>
 
 #include "axon_device.cuh"
+#include "batch_common.cuh"
 #include "plain.cuh"
 #include "emit.cuh"
 #include "learn.cuh"
@@ -27,54 +32,78 @@
 
 namespace axon {
 
-template <int CPW>
+// LEARN is c.learn as a template argument: readout launches carry none of the learning
+// code's register pressure.
+template <int CPW, bool LEARN>
 __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
   extern __shared__ __align__(16) uint32_t sm[];
   const uint32_t ncol = c.ncol, incols = c.incols;
   const uint32_t ngrp = ncol / 8u, nactw = (((ngrp + 31u) / 32u) + 3u) & ~3u;  // 16-byte multiple
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, wpb = blockDim.x >> 5;
+  const uint32_t maxCols = wpb * CPW;      // columns owned by this CTA
+  const PresentSmem L = present_smem_layout(ncol, incols, CPW);
   uint32_t* sSpk0 = sm;                    // spike vectors, ping-pong
   uint32_t* sSpk1 = sm + ncol;
   uint32_t* sAct0 = sm + 2 * ncol;         // group-activity bits, ping-pong
   uint32_t* sAct1 = sAct0 + nactw;
-  uint32_t* sD = sAct1 + nactw;            // staged drives of the current step
-  uint32_t* sB = sD + ncol;                // staged ungated ballots
-  uint32_t* sStim = sB + ncol;             // input clamp pattern
-  uint32_t* sHist = sStim + ((incols + 3u) & ~3u);  // 256 bins of the threshold select
-  uint32_t* sRed = sHist + 256;            // 192 words of reduction scratch
-  uint32_t* sFlag = sRed + 192;            // [0] barrier flag, [1] learning-task count
-  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, wpb = blockDim.x >> 5;
-  const uint32_t maxCols = wpb * CPW;      // columns owned by this CTA
-  uint32_t* sTask = sFlag + 4;             // learning tasks: (column slot << 5) | branch
+  uint32_t* sStim = sAct1 + nactw;         // input clamp pattern
+  uint32_t* sHist = sStim + ((incols + 3u) & ~3u);  // the step's drive histogram (kHistWords)
+  uint32_t* sFlag = sHist + kHistWords;    // [0] barrier flag, [1] learning-task count, [2] candidates,
+                                           // [3] tile-pool slots claimed, [4..7] threshold select
+  uint64_t* sMbar = reinterpret_cast<uint64_t*>(sFlag + 16);  // one per column slot (tile pool)
+  uint32_t* sTask = sFlag + 16 + 2 * kMaxColSlots;  // learning tasks: (column slot << 5) | branch
   uint32_t* sBBL = sTask + maxCols * 32;   // branch-NMDA masks of the learning columns
   uint32_t* sLTP = sBBL + maxCols * 32;    // per-neuron potentiation counts of this step
   uint32_t* sLTD = sLTP + maxCols * 32;    // per-neuron depression counts
   uint32_t* sFiredL = sLTD + maxCols * 32; // spike ballot of each learning column
   uint32_t* sColL = sFiredL + maxCols;     // its column index
   uint32_t* sMark = sColL + maxCols;       // step+1 when the slot learns this step
+  uint32_t* sBias = sMark + maxCols;       // intrinsic bias of each owned neuron (slot * 32 + lane)
+  uint32_t* sMul = sBias + maxCols * 32;   // assembly multiplicity of each owned neuron
+  uint32_t* sRef = sMul + maxCols * 32;    // reference ball of each owned column
+  // phase A's tile pool; phase B reuses its start for the staged drives, the ungated
+  // ballots and the threshold candidates
+  uint4* sPool = reinterpret_cast<uint4*>(sm + L.poolWord);
+  const uint32_t poolTiles = L.poolTiles;
+  uint32_t* sD = sm + L.poolWord;          // staged drives of the current step
+  uint32_t* sB = sD + ncol;                // staged ungated ballots
+  uint32_t* sCand = sB + ncol;             // drives of the threshold's histogram bin (up to ncol)
 
   const uint32_t gwarp = blockIdx.x * wpb + warp, nwarps = gridDim.x * wpb;
+  uint32_t* xhist = d.bar + 64;            // step t counts its recurrent drives into histogram t mod 3
+  // branch term of k_drive (src/axon.mm:174-178): the count (modes 0, 1) plus, when the
+  // branch reaches dthr, the boost (mode 1) or 1 (mode 2)
+  const uint32_t linMask = c.mode != 2u ? kFull : 0u;
+  const uint32_t addN = c.mode == 1u ? c.boost : (c.mode == 2u ? 1u : 0u);
 
   for (uint32_t i = tid; i < ncol; i += blockDim.x) sSpk0[i] = 0u;
   for (uint32_t i = tid; i < nactw; i += blockDim.x) sAct0[i] = 0u;
   for (uint32_t i = tid; i < maxCols; i += blockDim.x) sMark[i] = 0u;
-  if (tid == 0) sFlag[1] = 0u;
+  if (tid == 0) {
+    sFlag[1] = 0u;
+    sFlag[3] = 0u;
+    for (uint32_t i = 0; i < maxCols; ++i) mbar_init(&sMbar[i], 1);
+    fence_proxy_async_smem();
+  }
   for (uint32_t i = tid; i < incols; i += blockDim.x) sStim[i] = d.stim[i];
 
-  // per-column state of the columns this warp owns (lane = neuron, or lane = branch for conn)
-  uint32_t col[CPW], cn[CPW], bias[CPW], mul[CPW], refb[CPW], acc[CPW], bb[CPW], ball[CPW], vk[CPW], vk1[CPW], drv[CPW];
+  // the columns this warp owns and their conn rows (lane = branch) stay in registers; the
+  // rest of their per-neuron state lives in shared memory by column slot (warp * CPW + i)
+  uint32_t col[CPW], cn[CPW];
+  uint32_t mph = 0;  // bit i: phase parity of column slot i's mbarrier
 #pragma unroll
   for (int i = 0; i < CPW; ++i) {
     col[i] = gwarp + (uint32_t)i * nwarps;
-    cn[i] = bias[i] = mul[i] = refb[i] = acc[i] = bb[i] = ball[i] = vk[i] = vk1[i] = drv[i] = 0u;
+    cn[i] = 0u;
+    const uint32_t slot = warp * CPW + (uint32_t)i;
     if (col[i] < ncol) {
       cn[i] = d.conn[col[i] * kNslot + lane];
-      bias[i] = d.bias[col[i] * 32u + lane];
-      mul[i] = d.mult[col[i] * 32u + lane];
-      refb[i] = d.refBall[col[i]];
+      sBias[slot * 32u + lane] = d.bias[col[i] * 32u + lane];
+      sMul[slot * 32u + lane] = d.mult[col[i] * 32u + lane];
+      if (lane == 0) sRef[slot] = d.refBall[col[i]];
     }
   }
   __syncthreads();
-  uint32_t thPrev = 0;  // last step's threshold: a starting guess for the next selection
 
   for (uint32_t t = 0; t < c.T; ++t) {
     const uint32_t* sIn = (t & 1u) ? sSpk1 : sSpk0;
@@ -84,58 +113,105 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
     const uint4* sIn4 = reinterpret_cast<const uint4*>(sIn);
     const uint32_t par = t & 1u;
     const bool clamp = t < c.clampSteps;
-    const uint32_t phase = (!c.learn || !c.contrast) ? 0u
+    const uint32_t phase = (!LEARN || !c.contrast) ? 0u
                            : (clamp ? 1u : (((t - c.clampSteps) % c.ltdEvery == 0u) ? 2u : 3u));
+    // what phase A leaves for phase C of the same step
+    uint32_t acc[CPW], bb[CPW], vk[CPW], vk1[CPW];
+#pragma unroll
+    for (int i = 0; i < CPW; ++i) acc[i] = bb[i] = vk[i] = vk1[i] = 0u;
 
     // per-phase device timer stamps of the profile mode (thread 0 of every CTA)
     unsigned long long* stamp = d.prof ? d.prof + ((size_t)t * gridDim.x + blockIdx.x) * 5u : nullptr;
     if (stamp && tid == 0) stamp[0] = globaltimer_ns();
     // ---------------- phase A: drive (k_drive, src/axon.mm:150-190) + ungated k-WTA
-    // The owner warp walks its column's non-silent branches four at a time, so four W3
-    // tiles (2 x 512 B each) are in flight per warp; spikes come from shared memory.
+    // The owner warp claims one pool slot per non-silent branch of its column; the lane of
+    // each such branch issues the tile's bulk copy, so all of the CTA's tiles are in flight
+    // together. A column whose claim does not fit the pool streams its tiles through
+    // registers instead, four at a time. Spikes come from shared memory.
 #pragma unroll
     for (int i = 0; i < CPW; ++i) {
       if (col[i] >= ncol) continue;  // warp-uniform
       const uint32_t cc = col[i];
-      uint32_t active = __ballot_sync(kFull, (sActIn[cn[i] >> 5] >> (cn[i] & 31u)) & 1u);
+      const bool on = (sActIn[cn[i] >> 5] >> (cn[i] & 31u)) & 1u;
+      uint32_t active = __ballot_sync(kFull, on);
+      const uint32_t n = (uint32_t)__popc(active);
       uint32_t a = 0, b2 = 0;
-      const uint4* Wt = d.W3 + (size_t)cc * kNslot * kTileU4 + lane;
-      while (active) {
-        uint32_t s[4];
-        bool v[4];
-        uint4 w0[4], w1[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          v[u] = active != 0u;
-          s[u] = v[u] ? (uint32_t)(__ffs(active) - 1) : 0u;
-          active &= active - 1u;
+      uint32_t slot0 = 0;
+      if (lane == 0 && n != 0u) slot0 = atomicAdd(sFlag + 3, n);
+      slot0 = __shfl_sync(kFull, slot0, 0);
+      if (n != 0u && slot0 + n <= poolTiles) {
+        uint64_t* mb = &sMbar[warp * CPW + (uint32_t)i];
+        if (lane == 0) mbar_expect_tx(mb, n * 1024u);
+        __syncwarp();
+        if (on) {
+          const uint32_t r = (uint32_t)__popc(active & ((1u << lane) - 1u));
+          fence_proxy_async_smem();
+          bulk_g2s(sPool + (size_t)(slot0 + r) * kTileU4, d.W3 + ((size_t)cc * kNslot + lane) * kTileU4, 1024u, mb);
         }
+        const uint32_t ph = (mph >> i) & 1u;
+        if (!mbar_wait(mb, ph, c.waitNs)) {
+          // the copies did not land in time: record it, wait (bounded) for them, and let
+          // the grid barrier end the launch
+          if (lane == 0) atomicCAS(d.err, 0u, kErrTimeout);
+          mbar_wait(mb, ph, c.waitNs > kDrainNs ? c.waitNs : kDrainNs);
+        }
+        mph ^= 1u << i;
+        const uint4* T = sPool + (size_t)slot0 * kTileU4 + lane;
+        for (uint32_t r = 0; active; ++r, T += kTileU4) {
+          const uint32_t s = (uint32_t)(__ffs(active) - 1);
+          active &= active - 1u;
+          const uint32_t g = __shfl_sync(kFull, cn[i], s);
+          const uint32_t cnt = popc4(T[0], sIn4[2 * g]) + popc4(T[32], sIn4[2 * g + 1]);
+          const bool nmda = cnt >= c.dthr;
+          if (nmda) b2 |= 1u << s;
+          a += (cnt & linMask) + (nmda ? addN : 0u);
+        }
+      } else {
+        const uint4* Wt = d.W3 + (size_t)cc * kNslot * kTileU4 + lane;
+        while (active) {
+          uint32_t s[4];
+          bool v[4];
+          uint4 w0[4], w1[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (v[u]) {
-            w0[u] = __ldcg(Wt + s[u] * kTileU4);
-            w1[u] = __ldcg(Wt + s[u] * kTileU4 + 32);
+          for (int u = 0; u < 4; ++u) {
+            v[u] = active != 0u;
+            s[u] = v[u] ? (uint32_t)(__ffs(active) - 1) : 0u;
+            active &= active - 1u;
           }
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (v[u]) {
-            const uint32_t g = __shfl_sync(kFull, cn[i], s[u]);
-            const uint32_t cnt = popc4(w0[u], sIn4[2 * g]) + popc4(w1[u], sIn4[2 * g + 1]);
-            const bool nmda = cnt >= c.dthr;
-            if (nmda) b2 |= 1u << s[u];
-            a += c.mode == 0u ? cnt : (c.mode == 1u ? (nmda ? cnt + c.boost : cnt) : (nmda ? 1u : 0u));
-          }
+          for (int u = 0; u < 4; ++u)
+            if (v[u]) {
+              w0[u] = __ldcg(Wt + s[u] * kTileU4);
+              w1[u] = __ldcg(Wt + s[u] * kTileU4 + 32);
+            }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (v[u]) {
+              const uint32_t g = __shfl_sync(kFull, cn[i], s[u]);
+              const uint32_t cnt = popc4(w0[u], sIn4[2 * g]) + popc4(w1[u], sIn4[2 * g + 1]);
+              const bool nmda = cnt >= c.dthr;
+              if (nmda) b2 |= 1u << s[u];
+              a += (cnt & linMask) + (nmda ? addN : 0u);
+            }
+        }
       }
       if (c.facil != 0u && ((sIn[cc] >> lane) & 1u)) a += c.facil;
-      const uint32_t bi = c.useBias ? (bias[i] >> c.biasShift) : 0u;
+      const uint32_t bi = c.useBias ? (sBias[(warp * CPW + (uint32_t)i) * 32u + lane] >> c.biasShift) : 0u;
       a = a > bi ? a - bi : 0u;
       acc[i] = a;
       bb[i] = b2;
-      drv[i] = __reduce_add_sync(kFull, a);
-      ball[i] = warp_kwta(a, lane, c.k, vk[i], vk1[i]);
+      const uint32_t drv = __reduce_add_sync(kFull, a);
+      const uint32_t ball = warp_kwta(a, lane, c.k, vk[i], vk1[i]);
       if (lane == 0) {
-        __stcg(d.xdrive + par * ncol + cc, drv[i]);
-        __stcg(d.xball + par * ncol + cc, ball[i]);
+        __stcg(d.xdrive + par * ncol + cc, drv);
+        __stcg(d.xball + par * ncol + cc, ball);
+        if (cc >= incols && drv < (1u << 24)) {
+          uint32_t* h = xhist + (t % 3u) * kHistWords + theta_key(drv);
+          atomicAdd(h, 1u);
+          atomicMax(h + kThetaBins, drv);
+          atomicMax(h + 2u * kThetaBins, ~drv);
+        }
+        if (t + 1u == c.T) d.drive[cc] = drv;  // final state: the last step's column drive
       }
     }
 
@@ -147,18 +223,23 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
     if (stamp && tid == 0) stamp[2] = globaltimer_ns();
 
     // ---------------- phase B: column threshold (k_topk) and the full spike vector
-    // drives and ballots come from L2 by asynchronous copies; the ballots keep arriving
-    // while the threshold is selected from the drives
+    // drives, this step's drive histogram and the ballots come from L2 by asynchronous
+    // copies; the ballots keep arriving while the threshold is selected
     for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x)
       cp_async16(reinterpret_cast<uint4*>(sD) + i, reinterpret_cast<const uint4*>(d.xdrive + par * ncol) + i);
+    for (uint32_t i = tid; i < kHistWords / 4u; i += blockDim.x)
+      cp_async16(reinterpret_cast<uint4*>(sHist) + i, reinterpret_cast<const uint4*>(xhist + (t % 3u) * kHistWords) + i);
     cp_async_commit();
     for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x)
       cp_async16(reinterpret_cast<uint4*>(sB) + i, reinterpret_cast<const uint4*>(d.xball + par * ncol) + i);
     cp_async_commit();
+    if (tid == 0) { sFlag[2] = 0u; sFlag[3] = 0u; }  // every warp has claimed its pool slots
+    // histogram t+2 (last read in step t-1, before this barrier) is cleared for its next use
+    if (blockIdx.x == 0 && t >= 1u)
+      for (uint32_t i = tid; i < kHistWords; i += blockDim.x) __stcg(xhist + ((t + 2u) % 3u) * kHistWords + i, 0u);
     cp_async_wait<1>();
     __syncthreads();
-    const uint32_t theta = block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed, thPrev);
-    thPrev = theta;
+    const uint32_t theta = hist_theta(sD, sHist, sCand, sFlag + 2, incols, ncol, c.targetCols, c.topkPar);
     const uint32_t gate = max(theta, 1u);
     cp_async_wait<0>();
     __syncthreads();
@@ -172,14 +253,20 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
     for (int i = 0; i < CPW; ++i) {
       if (col[i] >= ncol) continue;
       const uint32_t cc = col[i];
+      const uint32_t slot = warp * CPW + (uint32_t)i;
       const uint32_t b = sOut[cc];
       const bool recur = cc >= incols;
       const bool fired = (b >> lane) & 1u;
+      if (t + 1u == c.T) {  // final state of the owned neurons, as present() leaves it
+        d.acc[cc * 32u + lane] = acc[i];
+        d.bbits[cc * 32u + lane] = bb[i];
+        if (lane == 0) d.marg[cc] = vk[i] > vk1[i] ? 1u : 0u;
+      }
       if (recur) {
         // stats[2] and driveLog, src/axon.mm:213-220
         const uint32_t coinc = __reduce_add_sync(kFull, fired ? (uint32_t)__popc(bb[i]) : 0u);
-        const bool member = (refb[i] >> lane) & 1u;
-        const bool shared = mul[i] > 1u;
+        const bool member = (sRef[slot] >> lane) & 1u;
+        const bool shared = sMul[slot * 32u + lane] > 1u;
         const uint32_t mS = __ballot_sync(kFull, member && shared), mE = __ballot_sync(kFull, member && !shared);
         const uint32_t sumS = __reduce_add_sync(kFull, (member && shared) ? acc[i] : 0u);
         const uint32_t sumE = __reduce_add_sync(kFull, (member && !shared) ? acc[i] : 0u);
@@ -202,18 +289,17 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
           if (vk[i] == 0u) atomicAdd(d.stats + sb + 4u, 1u);
         }
       }
-      if (!c.learn) continue;
+      if (!LEARN) continue;
       // k_bias, src/axon.mm:240-253
       if (recur) {
         const int dec = ((t % max(c.biasDownEvery, 1u)) == 0u) ? (int)c.biasDown : 0;
-        const int nb = (int)bias[i] + (fired ? (int)c.biasUp : -dec);
-        bias[i] = (uint32_t)max(0, nb);
+        const int nb = (int)sBias[slot * 32u + lane] + (fired ? (int)c.biasUp : -dec);
+        sBias[slot * 32u + lane] = (uint32_t)max(0, nb);
       }
       // k_learn, src/axon.mm:436-495: each voted branch of a learning column becomes a
       // task that any warp of the CTA runs, so a column's read-modify-writes overlap
       if (phase == 3u || b == 0u) continue;
       if (c.marginGate != 0u && !(vk[i] > vk1[i])) continue;
-      const uint32_t slot = warp * CPW + (uint32_t)i;
       const uint32_t vmask = __reduce_or_sync(kFull, fired ? bb[i] : 0u);
       sBBL[slot * 32u + lane] = bb[i];
       sLTP[slot * 32u + lane] = 0u;
@@ -221,7 +307,7 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
       if (lane == 0) { sFiredL[slot] = b; sColL[slot] = cc; sMark[slot] = t + 1u; }
       if ((vmask >> lane) & 1u) sTask[atomicAdd(sFlag + 1, 1u)] = (slot << 5) | lane;
     }
-    if (c.learn) {
+    if (LEARN) {
       __syncthreads();
       const uint32_t ntask = sFlag[1];
       for (uint32_t k = warp; k < ntask; k += wpb) {
@@ -289,12 +375,8 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
   for (int i = 0; i < CPW; ++i) {
     if (col[i] >= ncol) continue;
     const uint32_t cc = col[i];
-    d.acc[cc * 32u + lane] = acc[i];
-    d.bbits[cc * 32u + lane] = bb[i];
-    if (c.learn) d.bias[cc * 32u + lane] = bias[i];
+    if (LEARN) d.bias[cc * 32u + lane] = sBias[(warp * CPW + (uint32_t)i) * 32u + lane];
     if (lane == 0) {
-      d.drive[cc] = drv[i];
-      d.marg[cc] = vk[i] > vk1[i] ? 1u : 0u;
       gLast[cc] = sLast[cc];
       gPrev[cc] = T >= 2u ? sPrev[cc] : 0u;
       if (d.finalOut) d.finalOut[cc] = sLast[cc];
@@ -304,34 +386,44 @@ __global__ void __launch_bounds__(1024, 1) k_present(NetDev d, PresentCfg c) {
 
 // ---------------------------------------------------------------- launch helpers
 size_t present_smem_bytes(uint32_t ncol, uint32_t incols, int cpw) {
-  const uint32_t ngrp = ncol / 8u, nactw = (((ngrp + 31u) / 32u) + 3u) & ~3u;
-  const size_t maxCols = 32ull * cpw;  // upper bound of wpb * cpw
-  const size_t words = 2ull * ncol + 2ull * nactw + 2ull * ncol + ((incols + 3u) & ~3u) + 256 + 192 + 4 +
-                       maxCols * (4 * 32 + 3);
-  return words * 4;
+  return present_smem_layout(ncol, incols, cpw).bytes;
+}
+
+static const void* present_fn(int cpw, bool learn) {
+  switch (cpw) {
+    case 1: return learn ? (const void*)k_present<1, true> : (const void*)k_present<1, false>;
+    case 2: return learn ? (const void*)k_present<2, true> : (const void*)k_present<2, false>;
+    default: return nullptr;
+  }
 }
 
 cudaError_t launch_present(const NetDev& d, const PresentCfg& c, const LaunchShape& ls, cudaStream_t st) {
   void* args[] = {(void*)&d, (void*)&c};
-  const void* fn = nullptr;
-  switch (ls.cpw) {
-    case 1: fn = (const void*)k_present<1>; break;
-    case 2: fn = (const void*)k_present<2>; break;
-    default: return cudaErrorInvalidValue;
-  }
+  const void* fn = present_fn(ls.cpw, c.learn != 0u);
+  if (!fn) return cudaErrorInvalidValue;
+  // barrier counter and the three drive histograms start at zero
+  const cudaError_t e = cudaMemsetAsync(d.bar, 0, kBarRegionWords * 4u, st);
+  if (e != cudaSuccess) return e;
   return cudaLaunchCooperativeKernel(fn, dim3(ls.grid), dim3(ls.wpb * 32), args, ls.smem, st);
 }
 
+// Sets the shared-memory size of both forms (learning, readout) and returns the smaller
+// number of co-resident blocks per SM.
 cudaError_t present_max_blocks_per_sm(int cpw, int threads, size_t smem, int* out) {
-  const void* fn = nullptr;
-  switch (cpw) {
-    case 1: fn = (const void*)k_present<1>; break;
-    case 2: fn = (const void*)k_present<2>; break;
-    default: return cudaErrorInvalidValue;
+  *out = 0;
+  int best = 1 << 30;
+  for (bool learn : {false, true}) {
+    const void* fn = present_fn(cpw, learn);
+    if (!fn) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int n = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, smem);
+    if (e != cudaSuccess) return e;
+    best = n < best ? n : best;
   }
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, fn, threads, smem);
+  *out = best;
+  return cudaSuccess;
 }
 
 // ---------------------------------------------------------------- init kernels

@@ -110,7 +110,6 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
       if (!dStats) CK(cudaMemsetAsync(statsTmp, 0, 1024 * 4, stream));
       if (dLog) dd.driveLog = dLog + (size_t)b * 256;
       dd.finalOut = dFinal ? dFinal + (size_t)b * ncol : nullptr;
-      CK(cudaMemsetAsync(d.bar, 0, 4, stream));
       CK(launch_present(dd, pc, shape, stream));
     }
     CK(cudaEventRecord(ev1, stream));

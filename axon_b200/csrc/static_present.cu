@@ -30,8 +30,9 @@ using namespace axon;
 namespace {
 
 constexpr uint32_t kStaticMaxNcol = 4096;
-// 2 x ncol drive slots + 2 x ncol ballot slots + 64-word control block (barrier, error)
-constexpr uint32_t kStaticScratchWords = 4 * kStaticMaxNcol + 64;
+// 2 x ncol drive slots + 2 x ncol ballot slots + the barrier region (barrier, error word at
+// +16, drive histograms at +64)
+constexpr uint32_t kStaticScratchWords = 4 * kStaticMaxNcol + kBarRegionWords;
 
 static __device__ __align__(256) uint32_t g_present_scratch[kStaticScratchWords];
 
@@ -126,8 +127,8 @@ extern "C" axon_status axon_present_static(const axon_cfg* cfg, const axon_state
   }
   if (!ok) return set_error(AXON_EINVAL, "no co-resident launch shape for this ncol");
 
-  // clear what the kernel expects at zero: barrier counter, error word, stats
-  CK(cudaMemsetAsync(d.bar, 0, 64 * 4, 0));
+  // clear what the kernel expects at zero: stats (launch_present clears the barrier
+  // region, error word included)
   CK(cudaMemsetAsync(d.stats, 0, 1024 * 4, 0));
   CK(launch_present(d, p, ls, 0));
   CK(cudaStreamSynchronize(0));

@@ -108,4 +108,111 @@ static __device__ __noinline__ uint32_t block_theta(const uint32_t* sD, uint32_t
   return max(prefix + lo, 1u);
 }
 
+// Bin of a column drive d < 2^24 in the threshold histogram: monotone in d, the drive
+// itself below 64, and above that the octave with the five bits after the leading one
+// (32 bins per octave, 640 bins in all). Bin k >= 64 holds the drives
+// [(32 | (k & 31)) << b, ((32 | (k & 31)) + 1) << b) with b = (k >> 5) - 1.
+__device__ __forceinline__ uint32_t theta_key(uint32_t d) {
+  if (d < 64u) return d;
+  const uint32_t e = 31u - __clz(d);  // 6..23
+  return ((e - 4u) << 5) | ((d >> (e - 5u)) & 31u);
+}
+
+// The same threshold as block_theta (src/axon.mm:301-352 and :259-292) when every
+// recurrent drive below 2^24 has been recorded in sH as it was published: per theta_key
+// bin the count (sH[0, 640)), the largest drive (sH[640, 1280)) and the complement of the
+// smallest (sH[1280, 1920)). Warp 0 scans the counts from the top to the bin that holds
+// the need-th largest drive. That drive is the bin itself below 64, and the bin's largest
+// or smallest drive when it ranks first or last in its bin; otherwise the block collects
+// the bin's drives (usually a few) into sCand and warp 0 resolves the rank bit by bit, most
+// significant first. sCtl[0] is the candidate counter and must be zero on entry;
+// sCtl[2..5] is scratch. Every thread of the block calls it.
+static __device__ __forceinline__ uint32_t hist_theta(const uint32_t* sD, const uint32_t* sH, uint32_t* sCand,
+                                                   uint32_t* sCtl, uint32_t incols, uint32_t ncol, uint32_t need,
+                                                   uint32_t topkPar) {
+  constexpr uint32_t kPer = 20;  // bins per lane (640 / 32)
+  constexpr uint32_t kThetaBinCount = 32u * kPer;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  if (warp == 0u) {
+    uint32_t h[kPer], ls = 0;
+    const uint4* h4 = reinterpret_cast<const uint4*>(sH + lane * kPer);
+#pragma unroll
+    for (int i = 0; i < (int)kPer / 4; ++i) {
+      const uint4 v = h4[i];
+      h[4 * i] = v.x; h[4 * i + 1] = v.y; h[4 * i + 2] = v.z; h[4 * i + 3] = v.w;
+      ls += v.x + v.y + v.z + v.w;
+    }
+    uint32_t S = ls;  // drives in the bins of this lane and the lanes above
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t v = __shfl_down_sync(kFull, S, off);
+      if (lane + off < 32u) S += v;
+    }
+    const uint32_t count = __shfl_sync(kFull, S, 0), zeros = __shfl_sync(kFull, h[0], 0);
+    uint32_t res = 0;  // the threshold when it is known without candidates (always >= 1), else 0
+    uint32_t b = 0, above = 0, inBin = 0;
+    if (need == 0u) {
+      res = topkPar ? 1u : 0xFFFFFFu;
+    } else if (count < need || count - zeros < need) {
+      res = 1u;
+    } else {
+      uint32_t Snext = __shfl_down_sync(kFull, S, 1);
+      if (lane == 31u) Snext = 0u;
+      const bool mine = S >= need && Snext < need;
+      if (mine) {
+        uint32_t cum = Snext;
+#pragma unroll
+        for (int i = (int)kPer - 1; i >= 0; --i) {
+          if (cum + h[i] >= need) { b = lane * kPer + (uint32_t)i; above = cum; inBin = h[i]; break; }
+          cum += h[i];
+        }
+      }
+      const uint32_t src = (uint32_t)__ffs(__ballot_sync(kFull, mine)) - 1u;
+      b = __shfl_sync(kFull, b, src);
+      above = __shfl_sync(kFull, above, src);
+      inBin = __shfl_sync(kFull, inBin, src);
+      if (b < 64u) res = b;  // one drive per bin; b >= 1 because at least `need` drives are positive
+      else if (need - above == 1u) res = sH[kThetaBinCount + b];
+      else if (need - above == inBin) res = ~sH[2u * kThetaBinCount + b];
+    }
+    if (lane == 0u) { sCtl[2] = res; sCtl[3] = b; sCtl[4] = need - above; sCtl[5] = inBin; }
+  }
+  __syncthreads();
+  const uint32_t res = sCtl[2];
+  if (res != 0u) return res;
+  const uint32_t b = sCtl[3];
+  const uint32_t bits = (b >> 5) - 1u, lo = (32u | (b & 31u)) << bits;
+  for (uint32_t c = incols + threadIdx.x; c < ncol; c += blockDim.x) {
+    const uint32_t d = sD[c];
+    if (d < (1u << 24) && theta_key(d) == b) sCand[atomicAdd(sCtl, 1u)] = d - lo;
+  }
+  __syncthreads();
+  if (warp == 0u) {
+    uint32_t rem = sCtl[4];  // rank of the answer among the drives of bin b, from the top
+    const uint32_t inBin = sCtl[5];
+    uint32_t prefix = 0;
+    if (inBin <= 64u) {
+      const bool v0 = lane < inBin, v1 = lane + 32u < inBin;
+      const uint32_t x0 = v0 ? sCand[lane] : 0u, x1 = v1 ? sCand[lane + 32u] : 0u;
+      for (int bit = (int)bits - 1; bit >= 0; --bit) {
+        const uint32_t want = (prefix >> bit) | 1u;
+        const uint32_t c1 = (uint32_t)__popc(__ballot_sync(kFull, v0 && (x0 >> bit) == want)) +
+                            (uint32_t)__popc(__ballot_sync(kFull, v1 && (x1 >> bit) == want));
+        if (c1 >= rem) prefix |= 1u << bit; else rem -= c1;
+      }
+    } else {
+      for (int bit = (int)bits - 1; bit >= 0; --bit) {
+        const uint32_t want = (prefix >> bit) | 1u;
+        uint32_t c1 = 0;
+        for (uint32_t i = lane; i < inBin; i += 32u) c1 += (sCand[i] >> bit) == want;
+        c1 = __reduce_add_sync(kFull, c1);
+        if (c1 >= rem) prefix |= 1u << bit; else rem -= c1;
+      }
+    }
+    if (lane == 0u) sCtl[2] = lo + prefix;
+  }
+  __syncthreads();
+  return sCtl[2];
+}
+
 }  // namespace axon

@@ -177,7 +177,7 @@ axon_status axon_recall_device(axon_net* net, const uint32_t* cues, uint32_t B, 
  * owns, passed as device pointers with the sizes listed for axon_buf (plus stim: ncol
  * words, the clamp pattern). Allocates nothing - no cudaMalloc/cudaFree, no library
  * allocation: the kernel's only scratch is a fixed device array in the library sized for
- * ncol <= 4096 (about 64 KiB per GPU, held until the process exits); larger ncol returns
+ * ncol <= 4096 (about 87 KiB per GPU, held until the process exits); larger ncol returns
  * AXON_EINVAL. Runs on the default stream and returns when the presentation is done.
  * The first call on a device resolves the array's device address; make it before any
  * stream capture. Calls that overlap on the GPU share that array and race: issue one at
