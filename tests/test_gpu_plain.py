@@ -204,3 +204,30 @@ def test_step_count_limits(T, clamp):
     planes_equal(gpu, cpu, f"T{T}")
     gpu.close()
     cpu.close()
+
+
+@pytest.mark.parametrize("target,inbr", [(1500, 4), (64, 32)])
+def test_dense_activity_overflows_tile_pool(target, inbr):
+    """Nearly every branch non-silent: a CTA's columns need far more W3 tiles than its
+    shared-memory tile pool holds, so most columns stream their tiles through registers,
+    and the threshold bin holds many drives. Learning and readout against the oracle."""
+    import axon_b200 as ax
+
+    cfg = make_cfg(ncol=4096, incols=512, inbr=inbr, target=target, k=24)
+    gpu = ax.Network(cfg)
+    cpu = O.OracleNet(cfg)
+    gpu.init(7)
+    cpu.init(7)
+    pats = ax.stimuli(7, 2, cfg.incols, 448)
+    for p in range(2):
+        stim = ax.load_stim(pats[p], 1.0, 1000 + p, cfg.ncol)
+        gpu.present(stim, 6, 3, True)
+        cpu.present(stim, 6, 3, True)
+        compare(gpu, cpu, BUFS_EACH_PRESENT + ["HIST"], T=6, where=f"dense learn p{p}")
+    planes_equal(gpu, cpu, "dense")
+    stim = ax.load_stim(pats[0], 0.5, 4400, cfg.ncol)
+    gpu.present(stim, 8, 3, False, True, 0)
+    cpu.present(stim, 8, 3, False, True, 0)
+    compare(gpu, cpu, BUFS_EACH_PRESENT + ["HIST"], T=8, where="dense readout")
+    gpu.close()
+    cpu.close()
