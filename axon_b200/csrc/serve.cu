@@ -22,6 +22,8 @@
 namespace axon {
 
 constexpr int kServeThreads = 256;
+constexpr int kEmitThreads = 1024;     // one trajectory per CTA at a time: a full SM's warps
+constexpr uint32_t kEmitChunk = 256;   // gated columns whose per-neuron drives are staged at once
 
 // Spike vectors and activity bits were written by the previous tick's emit kernel and are
 // read-only here, so they are read through the non-coherent L1 path.
@@ -101,16 +103,17 @@ __global__ void __launch_bounds__(kServeThreads, 3) k_serve_drive(ServeDev d, Se
   }
 }
 
-__global__ void __launch_bounds__(kServeThreads) k_serve_emit(ServeDev d, ServeCfg c) {
+__global__ void __launch_bounds__(kEmitThreads) k_serve_emit(ServeDev d, ServeCfg c) {
   extern __shared__ __align__(16) uint32_t sm[];
   const uint32_t ncol = c.ncol, incols = c.incols, ngrp = ncol / 8u;
   uint32_t* sD = sm;
   uint32_t* sSpk = sD + ncol;
-  uint32_t* sList = sSpk + ncol;
+  uint32_t* sList = sSpk + ncol;  // threshold candidates, then the gated columns
   uint32_t* sStim = sList + ncol;
   uint32_t* sHist = sStim + ((incols + 3u) & ~3u);
   uint32_t* sRed = sHist + 256;
-  uint32_t* sCnt = sRed + 192;
+  uint32_t* sAccS = sRed + 192;                    // per-neuron drives of up to kEmitChunk gated columns
+  uint32_t* sCnt = sAccS + kEmitChunk * 32u;       // [0] gated columns
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
   const uint32_t nent = d.counts[0];
   for (uint32_t ei = blockIdx.x; ei < nent; ei += gridDim.x) {
@@ -144,16 +147,28 @@ __global__ void __launch_bounds__(kServeThreads) k_serve_emit(ServeDev d, ServeC
     }
     __syncthreads();
     const uint32_t npend = sCnt[0];
-    const uint32_t* accW = base + serve_acc_off(ncol);
-    for (uint32_t p = warp; p < npend; p += nw) {  // exact k-of-32 of the gated columns
-      const uint32_t cc = sList[p];
-      const uint32_t a = c.acc32 ? __ldcg(accW + cc * 32u + lane)
-                                 : (uint32_t)__ldcg(reinterpret_cast<const unsigned short*>(accW) + cc * 32u + lane);
-      uint32_t vk, vk1;
-      const uint32_t ball = warp_kwta(a, lane, c.k, vk, vk1);
-      if (lane == 0) sSpk[cc] = ball;
+    // exact k-of-32 of the gated columns: their per-neuron drives are staged in shared
+    // memory, all copies of a chunk in flight at once, then each warp takes columns
+    const uint32_t rowB = c.acc32 ? 128u : 64u, pieces = rowB / 16u;
+    const char* accB = reinterpret_cast<const char*>(base + serve_acc_off(ncol));
+    for (uint32_t p0 = 0; p0 < npend; p0 += kEmitChunk) {
+      const uint32_t np = min(kEmitChunk, npend - p0);
+      for (uint32_t i = tid; i < np * pieces; i += blockDim.x) {
+        const uint32_t p = i / pieces, q = i - p * pieces;
+        cp_async16(reinterpret_cast<char*>(sAccS) + p * rowB + q * 16u, accB + (size_t)sList[p0 + p] * rowB + q * 16u);
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncthreads();
+      for (uint32_t p = warp; p < np; p += nw) {
+        const uint32_t cc = sList[p0 + p];
+        const uint32_t a = c.acc32 ? sAccS[p * 32u + lane] : (uint32_t)reinterpret_cast<const unsigned short*>(sAccS)[p * 32u + lane];
+        uint32_t vk, vk1;
+        const uint32_t ball = warp_kwta(a, lane, c.k, vk, vk1);
+        if (lane == 0) sSpk[cc] = ball;
+      }
+      __syncthreads();
     }
-    __syncthreads();
     uint32_t* spkOut = base + (e.tloc & 1u) * ncol;
     uint32_t* actOut = base + 2u * ncol + (e.tloc & 1u) * d.nactw;
     uint4* dst = e.done != 0xFFFFFFFFu ? reinterpret_cast<uint4*>(d.doneBuf + (size_t)e.done * ncol) : nullptr;
@@ -206,7 +221,7 @@ __global__ void __launch_bounds__(kServeThreads) k_serve_emit(ServeDev d, ServeC
 }
 
 size_t serve_emit_smem_bytes(uint32_t ncol, uint32_t incols) {
-  return (3ull * ncol + ((incols + 3u) & ~3u) + 256 + 192 + 4) * 4;
+  return (3ull * ncol + ((incols + 3u) & ~3u) + 256 + 192 + kEmitChunk * 32ull + 4) * 4;
 }
 
 cudaError_t serve_prepare(size_t emitSmem) {
@@ -238,7 +253,7 @@ cudaError_t launch_serve_drive(const ServeDev& d, const ServeCfg& c, int sms, bo
 cudaError_t launch_serve_emit(const ServeDev& d, const ServeCfg& c, int sms, size_t emitSmem, cudaStream_t st,
                               uint32_t nnets) {
   k_serve_zero_counts<<<16, 256, 0, st>>>(d, nnets, c.ncol / 8u);
-  k_serve_emit<<<sms * 6, kServeThreads, emitSmem, st>>>(d, c);
+  k_serve_emit<<<sms * 2, kEmitThreads, emitSmem, st>>>(d, c);
   return cudaGetLastError();
 }
 
