@@ -117,18 +117,22 @@ class Network:
 
     def recall(self, cues: np.ndarray, T: int, clamp_steps: int, use_bias: int = 0, method: str = "batched",
                hist: bool = False, stats: bool = False, ref_ball: np.ndarray | None = None,
-               drive_log: np.ndarray | None = None, graph: bool = False) -> dict:
+               drive_log: np.ndarray | None = None, graph: bool = False, final_out: np.ndarray | None = None) -> dict:
         """B readout trajectories (present() with learn=0 for each cue row) in one call.
 
         Returns {"final": (B, ncol), "hist": (B, T, ncol) | None, "stats": (B, 1024) | None,
-        "drive_log": (B, 256) | None, "gpu_ms": float}.
+        "drive_log": (B, 256) | None, "gpu_ms": float}. final_out, a C-contiguous uint32
+        (B, ncol) array (page-locked memory copies fastest), receives the final spikes in
+        place of a new array.
         """
         cues = np.ascontiguousarray(cues, dtype=np.uint32)
         B = cues.shape[0]
         assert cues.shape == (B, self.ncol)
         a = A.RecallArgs(T=T, clamp_steps=clamp_steps, use_bias=use_bias,
                          method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN, graph=int(graph))
-        out = {"final": np.empty((B, self.ncol), dtype=np.uint32),
+        if final_out is not None:
+            assert final_out.dtype == np.uint32 and final_out.shape == (B, self.ncol) and final_out.flags.c_contiguous
+        out = {"final": final_out if final_out is not None else np.empty((B, self.ncol), dtype=np.uint32),
                "hist": np.empty((B, T, self.ncol), dtype=np.uint32) if hist else None,
                "stats": np.empty((B, 1024), dtype=np.uint32) if stats else None,
                "drive_log": None}

@@ -435,11 +435,12 @@ def main() -> None:
 
     # end to end through the public C-ABI call with pinned host buffers
     h_cues = torch.from_numpy(cues.view(np.int32)).pin_memory().numpy().view(np.uint32)
+    h_final = torch.empty(cues.shape, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
     e2e_t = []
     for it in range(0 if args.no_e2e else args.warmup + max(3, args.steps // 2)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r = net.recall(h_cues, T_RECALL, CLAMP_RECALL, graph=True)
+        r = net.recall(h_cues, T_RECALL, CLAMP_RECALL, graph=True, final_out=h_final)
         dt = time.perf_counter() - t0
         if it >= args.warmup:
             e2e_t.append(dt)
