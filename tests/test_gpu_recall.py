@@ -133,3 +133,20 @@ def test_graph_replay_equals_direct_launch():
     after = gpu.recall(cues, 20, 5, hist=True)
     g3 = gpu.recall(cues, 20, 5, hist=True, graph=True)
     assert np.array_equal(g3["hist"], after["hist"])
+
+
+def test_final_spikes_into_caller_array():
+    """final_out: the final spikes land in the caller's array (page-locked here, as a
+    serving host would pass it), equal to a recall that allocates its own result."""
+    import torch
+
+    cfg, gpu, cpu, pats = trained_pair({}, 3, 1, 16)
+    cues = make_cues(pats, cfg.ncol, 9, np.random.default_rng(4))
+    want = gpu.recall(cues, 12, 5)["final"]
+    buf = torch.zeros(cues.shape, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    for graph in (False, True, True):
+        r = gpu.recall(cues, 12, 5, graph=graph, final_out=buf)
+        assert r["final"] is buf and np.array_equal(buf, want)
+        buf[:] = 0
+    with pytest.raises(AssertionError):
+        gpu.recall(cues, 12, 5, final_out=np.zeros((cues.shape[0], cfg.ncol), dtype=np.int32))
