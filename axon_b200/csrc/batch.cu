@@ -45,7 +45,7 @@ cudaError_t launch_make_w3r(const uint4* W3, uint32_t* W3R, uint32_t ncol, cudaS
 }
 
 template <bool PACK, bool LIN>
-__global__ void __launch_bounds__(1024, 1) k_recall(RecallDev d, RecallCfg c) {
+__global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   extern __shared__ __align__(128) uint32_t sm[];
   const uint32_t ncol = c.ncol, incols = c.incols, B = c.B, ngrp = ncol / 8u;
   const uint32_t dthr = c.dthr, bst = c.bst;

@@ -156,7 +156,7 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     rd.bar = d.bar;
     rd.err = d.err;
     RecallShape rs{};
-    rs.threads = 1024;
+    rs.threads = 896;
     rs.smem = recall_smem_bytes(ncol, Bc, rc.acc32);
     int per_sm = 0;
     CK(recall_max_blocks_per_sm(rc.acc32, rs.threads, rs.smem, &per_sm));
