@@ -28,7 +28,7 @@ __host__ __device__ constexpr uint32_t sb_maxb() { return PACK ? kServeMaxB : kS
 }  // namespace
 
 template <bool PACK, bool LIN>
-__global__ void __launch_bounds__(1024, 1) k_serve_batched(ServeDev d, ServeCfg c) {
+__global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c) {
   extern __shared__ __align__(128) uint32_t sm[];
   const uint32_t ncol = c.ncol, ngrp = ncol / 8u, dthr = c.dthr, bst = c.bst;
   constexpr uint32_t accStride = sb_stride<PACK>();
@@ -253,7 +253,7 @@ cudaError_t serve_batched_prepare(uint32_t packed) {
 cudaError_t launch_serve_batched(const ServeDev& d, const ServeCfg& c, int sms, cudaStream_t st) {
   const uint32_t packed = (!c.acc32 && c.facil == 0u) ? 1u : 0u;
   void* args[] = {(void*)&d, (void*)&c};
-  return cudaLaunchKernel(sb_fn(packed, c.mode != 2u), dim3(sms), dim3(1024), args, serve_batched_smem_bytes(packed), st);
+  return cudaLaunchKernel(sb_fn(packed, c.mode != 2u), dim3(sms), dim3(896), args, serve_batched_smem_bytes(packed), st);
 }
 
 }  // namespace axon
