@@ -408,6 +408,7 @@ size_t multi_smem_bytes(uint32_t ncol, uint32_t incols, uint32_t maxCpw, int thr
 
 static const void* multi_fn(int threads, int tiles) {
   if (threads == 1024 && tiles == 4) return (const void*)k_multi<1024, 4>;
+  if (threads == 896 && tiles == 4) return (const void*)k_multi<896, 4>;
   if (threads == 512 && tiles == 8) return (const void*)k_multi<512, 8>;
   return nullptr;
 }

@@ -54,8 +54,8 @@ struct MultiCfg {
   uint64_t waitNs;
 };
 
-// Launch shape: (threads, tiles) is (1024, 4) or (512, 8), one CTA per SM; grid = CTAs of
-// all slots.
+// Launch shape: (threads, tiles) is (1024, 4), (896, 4) or (512, 8), one CTA per SM;
+// grid = CTAs of all slots.
 struct MultiShape {
   int threads, tiles, grid;
   size_t smem;

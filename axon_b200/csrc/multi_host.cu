@@ -396,7 +396,7 @@ axon_status MultiRun::tune(Shape* best, std::vector<std::vector<uint32_t>>* best
   std::vector<uint64_t> cost(n_);
   for (uint32_t i = 0; i < n_; ++i) cost[i] = plans_[i].steps;
   const uint32_t slotCands[] = {1, 2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 25, 32, 40, 50, 64, 74};
-  const int shapeCands[][2] = {{1024, 4}, {512, 8}};
+  const int shapeCands[][2] = {{1024, 4}, {896, 4}, {512, 8}};
   double bestT = 1e300;
   *tuneMs = 0.f;
   *tried = 0;
@@ -561,7 +561,7 @@ axon_status MultiRun::run(const uint32_t* seeds, const uint32_t* nstim, axon_mul
       R.tried = tried;
     } else {
       sh.slots = a_.slots ? std::min(a_.slots, n_) : std::min(n_, (uint32_t)net0_->sm_count);
-      sh.threads = a_.threads == 512 ? 512 : 1024;
+      sh.threads = (a_.threads == 512 || a_.threads == 896) ? (int)a_.threads : 1024;
       sh.tiles = sh.threads == 512 ? 8 : 4;
       if (sh.slots > (uint32_t)net0_->sm_count) return set_error(AXON_EINVAL, "more slots than SMs");
       ncta = split_ctas((uint32_t)net0_->sm_count, sh.slots);

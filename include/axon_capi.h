@@ -235,7 +235,7 @@ typedef struct axon_multi_args {
   uint32_t readout;     /* 1: run the readouts and fill results */
   uint32_t autotune;    /* 1: pick slots and CTA shape by timing candidates */
   uint32_t slots;       /* autotune == 0: concurrent networks (0 = one per network, at most one per SM) */
-  uint32_t threads;     /* autotune == 0: 1024 (4 W3 tiles in flight per warp) or 512 (8 tiles) */
+  uint32_t threads;     /* autotune == 0: 1024 or 896 (4 W3 tiles in flight per warp) or 512 (8 tiles) */
   uint32_t graph;       /* 1: launch through a captured CUDA graph */
   uint32_t method;      /* 0: one persistent launch, 1: plain path, one launch per presentation */
   uint32_t reserved[4]; /* zero */

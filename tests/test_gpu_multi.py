@@ -63,7 +63,7 @@ def test_one_launch_equals_plain_path(plain):
     assert_same(got, plain)
 
 
-@pytest.mark.parametrize("slots,threads", [(1, 1024), (2, 512), (5, 1024), (3, 512), (4, 1024)])
+@pytest.mark.parametrize("slots,threads", [(1, 1024), (2, 512), (5, 1024), (3, 512), (4, 1024), (3, 896), (5, 896)])
 def test_every_shape_gives_the_same_networks(plain, slots, threads):
     got = train("launch", autotune=False, slots=slots, threads=threads, graph=False)
     assert got[1]["slots"] == slots and got[1]["threads"] == threads
