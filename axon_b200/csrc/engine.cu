@@ -94,7 +94,7 @@ axon_status axon_net::create(const axon_cfg& c, int dev) {
   bool ok = false;
   for (int cpw : {1, 2}) {
     const uint32_t warps = (ncol + cpw - 1) / cpw;
-    int wpb = (int)std::min<uint32_t>(32, (warps + prop.multiProcessorCount - 1) / prop.multiProcessorCount);
+    int wpb = (int)std::min<uint32_t>(kPresentMaxWarps, (warps + prop.multiProcessorCount - 1) / prop.multiProcessorCount);
     wpb = std::max(wpb, 1);
     const int grid = (int)((warps + wpb - 1) / wpb);
     shape.smem = present_smem_bytes(ncol, c.incols, cpw);

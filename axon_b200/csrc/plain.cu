@@ -35,7 +35,7 @@ namespace axon {
 // LEARN is c.learn as a template argument: readout launches carry none of the learning
 // code's register pressure.
 template <int CPW, bool LEARN>
-__global__ void __launch_bounds__(896, 1) k_present(NetDev d, PresentCfg c) {
+__global__ void __launch_bounds__(kPresentMaxWarps * 32, 1) k_present(NetDev d, PresentCfg c) {
   extern __shared__ __align__(16) uint32_t sm[];
   const uint32_t ncol = c.ncol, incols = c.incols;
   const uint32_t ngrp = ncol / 8u, nactw = (((ngrp + 31u) / 32u) + 3u) & ~3u;  // 16-byte multiple

@@ -30,6 +30,7 @@ constexpr uint32_t kBarRegionWords = 64u + 3u * kHistWords;
 // pool of phase A, as large as the 227 KiB limit allows (at least the 3 x ncol words that
 // phase B stages into the same space).
 constexpr uint32_t kMaxColSlots = 64;      // column slots per CTA (32 warps x 2 columns)
+constexpr uint32_t kPresentMaxWarps = 28;  // k_present is compiled for 896 threads (72 registers)
 constexpr uint32_t kSmemLimitBytes = 227u * 1024u;
 struct PresentSmem {
   uint32_t poolWord;   // first word of the pool

@@ -114,7 +114,7 @@ extern "C" axon_status axon_present_static(const axon_cfg* cfg, const axon_state
   for (int cpw : {1, 2}) {
     const uint32_t warps = (ncol + cpw - 1) / cpw;
     int wpb = (int)((warps + sms - 1) / sms);
-    wpb = wpb < 1 ? 1 : (wpb > 32 ? 32 : wpb);
+    wpb = wpb < 1 ? 1 : (wpb > (int)kPresentMaxWarps ? (int)kPresentMaxWarps : wpb);
     const int grid = (int)((warps + wpb - 1) / wpb);
     ls.smem = present_smem_bytes(ncol, cfg->incols, cpw);
     int per_sm = 0;

@@ -154,10 +154,11 @@ def test_diagnostics_match_oracle():
         assert np.array_equal(gpu.wdiag(memb, asm, 3, sel), cpu.wdiag(memb, asm, 3, sel))
 
 
-@pytest.mark.parametrize("ncol", [8192])
+@pytest.mark.parametrize("ncol", [8192, 4608])
 def test_widest_network_two_columns_per_warp(ncol):
     """ncol 8,192, the widest network the engine takes, runs k_present with 2 columns per
-    warp (the grid must fit one wave of co-resident CTAs): learning and readout
+    warp (the grid must fit one wave of co-resident CTAs), and so does 4,608, where one
+    column per warp would need more than 28 warps per CTA: learning and readout
     presentations against the oracle; a wider network is refused at creation."""
     import axon_b200 as ax
 
