@@ -48,6 +48,14 @@ struct Done {
   std::vector<uint32_t> spk;
 };
 
+// A trajectory whose last step ran in the previous tick: its result is read back and
+// retired while the next tick runs.
+struct Finished {
+  axon_serve_result r;
+  uint32_t done;  // its row in the done buffer
+  uint32_t slot;
+};
+
 }  // namespace
 
 struct axon_server {
@@ -85,11 +93,17 @@ struct axon_server {
   // statistics
   uint64_t ticks = 0, sumActive = 0, maxActive = 0, completed = 0;
   double busy = 0, driveS = 0, emitS = 0;
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};  // per tick parity
+  // the previous tick, until its results are retired
+  std::vector<Finished> pending;
+  bool pendingTick = false;
+  uint32_t pendingNe = 0, pendingEv = 0;
+  size_t nRunning = 0;  // trajectories in the tables (nActive also counts those not yet retired)
 
   axon_status start(axon_net* const* ns, uint32_t n, uint64_t memBytes);
   void loop();
   axon_status tick();
+  axon_status retire_pending();
   void fail(axon_status s, const std::string& m) {
     std::lock_guard<std::mutex> g(mu);
     if (err == AXON_OK) { err = s; errMsg = m; }
@@ -161,7 +175,8 @@ axon_status axon_server::start(axon_net* const* ns, uint32_t n, uint64_t memByte
   CKS(cudaMallocHost(&hdone, (size_t)nslots * ncol * 4));
   CKS(cudaMallocHost((void**)&herr, 64));
   CKS(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-  for (auto& e : ev) CKS(cudaEventCreate(&e));
+  for (auto& evp : ev)
+    for (auto& e : evp) CKS(cudaEventCreate(&e));
   char* b = (char*)dmem;
   CKS(cudaMemsetAsync(b + listsOff, 0, n * listBytes + 256, stream));  // list lengths and error word start at zero
   std::vector<ServeNet> hn(n);
@@ -205,8 +220,9 @@ axon_server::~axon_server() {
   if (hmem) cudaFreeHost(hmem);
   if (hdone) cudaFreeHost(hdone);
   if (herr) cudaFreeHost(herr);
-  for (auto& e : ev)
-    if (e) cudaEventDestroy(e);
+  for (auto& evp : ev)
+    for (auto& e : evp)
+      if (e) cudaEventDestroy(e);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -249,9 +265,10 @@ axon_status axon_server::tick() {
       a.req.admit = t;
       act[a.req.net].push_back(std::move(a));
       ++nActive;
+      ++nRunning;
     }
   }
-  if (nActive == 0) return AXON_OK;
+  if (nRunning == 0) return retire_pending();
   // the tick's tables: every network's trajectories in batch-index order; a network with
   // many of them is advanced by the batched kernel, the others by the gather kernel
   entH.clear();
@@ -322,61 +339,85 @@ axon_status axon_server::tick() {
   td.cues = (const uint32_t*)(ds + oCue);
   td.par = par;
   CKS(cudaMemcpyAsync(ds, h, bytes, cudaMemcpyHostToDevice, stream));
-  CKS(cudaEventRecord(ev[0], stream));
+  const uint32_t eb = pendingEv ^ 1u;  // this tick's events (the previous tick's are still to be read)
+  CKS(cudaEventRecord(ev[eb][0], stream));
   CKS(launch_serve_drive(td, cfg, sms, ng > 0, nb > 0, stream));
-  CKS(cudaEventRecord(ev[1], stream));
+  CKS(cudaEventRecord(ev[eb][1], stream));
   CKS(launch_serve_emit(td, cfg, sms, emitSmem, stream, (uint32_t)nets.size()));
-  CKS(cudaEventRecord(ev[2], stream));
+  CKS(cudaEventRecord(ev[eb][2], stream));
+  // while the GPU runs this tick: the previous tick's results, from the host done buffer
+  // (its copy finished before this tick began), then this tick's read-backs into it
+  {
+    const axon_status st = retire_pending();
+    if (st != AXON_OK) return st;
+  }
   if (ndone) CKS(cudaMemcpyAsync(hdone, dev.doneBuf, (size_t)ndone * ncol * 4, cudaMemcpyDeviceToHost, stream));
   CKS(cudaMemcpyAsync(herr, dev.err, 4, cudaMemcpyDeviceToHost, stream));
-  CKS(cudaStreamSynchronize(stream));
-  const double t = now_s();
-  if (herr[0] != 0u) return set_error(AXON_ETIMEOUT, "a copy wait timed out in the serving kernel");
-  float msDrive = 0.f, msEmit = 0.f;
-  CKS(cudaEventElapsedTime(&msDrive, ev[0], ev[1]));
-  CKS(cudaEventElapsedTime(&msEmit, ev[1], ev[2]));
-  par ^= 1u;
-  // retire finished trajectories; the others keep their order (their next batch indices)
-  std::vector<Done> fin;
-  std::vector<uint32_t> freed;
+  // the trajectories whose last step runs now leave the tables (retired with the next
+  // tick); the others move one step on and keep their order (their next batch indices)
+  pending.clear();
   uint32_t ei = 0;
   for (std::vector<Active>& A : act) {
-    std::vector<Active> keep;
-    keep.reserve(A.size());
-    for (Active& a : A) {
+    size_t w = 0;
+    for (size_t i = 0; i < A.size(); ++i) {
+      Active& a = A[i];
       const ServeEntry& e = entH[ei++];
       if (e.done != 0xFFFFFFFFu) {
-        Done d;
-        d.r.tag = a.req.tag;
-        d.r.net = a.req.net;
-        d.r.steps = a.req.steps;
-        d.r.arrive_s = a.req.arrive;
-        d.r.admit_s = a.req.admit;
-        d.r.done_s = t;
-        const uint32_t* src = (const uint32_t*)hdone + (size_t)e.done * ncol;
-        d.spk.assign(src, src + ncol);
-        fin.push_back(std::move(d));
-        freed.push_back(a.slot);
+        Finished f{};
+        f.r.tag = a.req.tag;
+        f.r.net = a.req.net;
+        f.r.steps = a.req.steps;
+        f.r.arrive_s = a.req.arrive;
+        f.r.admit_s = a.req.admit;
+        f.done = e.done;
+        f.slot = a.slot;
+        pending.push_back(f);
       } else {
         ++a.tloc;
-        keep.push_back(std::move(a));
+        if (w != i) A[w] = std::move(a);
+        ++w;
       }
     }
-    A.swap(keep);
+    A.resize(w);
   }
-  {
-    std::lock_guard<std::mutex> g(mu);
-    for (auto& d : fin) done.push_back(std::move(d));
-    for (uint32_t s : freed) freeSlots.push_back(s);
-    nActive -= fin.size();
-    ++ticks;
-    driveS += msDrive * 1e-3;
-    emitS += msEmit * 1e-3;
-    sumActive += ne;
-    maxActive = std::max<uint64_t>(maxActive, ne);
-    completed += fin.size();
-    if (nActive == 0 && queue.empty()) cvIdle.notify_all();
+  nRunning -= pending.size();
+  pendingTick = true;
+  pendingNe = ne;
+  pendingEv = eb;
+  CKS(cudaStreamSynchronize(stream));
+  if (herr[0] != 0u) return set_error(AXON_ETIMEOUT, "a copy wait timed out in the serving kernel");
+  par ^= 1u;
+  return AXON_OK;
+}
+
+// Results of the previous tick: final spikes into the result queue, slots back to the
+// free list, the tick into the counters.
+axon_status axon_server::retire_pending() {
+  if (!pendingTick) return AXON_OK;
+  pendingTick = false;
+  const double t = now_s();
+  float msDrive = 0.f, msEmit = 0.f;
+  CKS(cudaEventElapsedTime(&msDrive, ev[pendingEv][0], ev[pendingEv][1]));
+  CKS(cudaEventElapsedTime(&msEmit, ev[pendingEv][1], ev[pendingEv][2]));
+  std::vector<Done> fin(pending.size());
+  for (size_t i = 0; i < pending.size(); ++i) {
+    fin[i].r = pending[i].r;
+    fin[i].r.done_s = t;
+    const uint32_t* src = (const uint32_t*)hdone + (size_t)pending[i].done * ncol;
+    fin[i].spk.assign(src, src + ncol);
   }
+  std::lock_guard<std::mutex> g(mu);
+  for (auto& d : fin) done.push_back(std::move(d));
+  for (const Finished& f : pending) freeSlots.push_back(f.slot);
+  nActive -= pending.size();
+  ++ticks;
+  driveS += msDrive * 1e-3;
+  emitS += msEmit * 1e-3;
+  sumActive += pendingNe;
+  maxActive = std::max<uint64_t>(maxActive, pendingNe);
+  completed += pending.size();
+  pending.clear();
+  if (nActive == 0 && queue.empty()) cvIdle.notify_all();
   return AXON_OK;
 }
 
