@@ -228,7 +228,6 @@ __global__ void __launch_bounds__(NT, 1) k_multi(MultiDev m, MultiCfg c) {
           uint32_t* dlog = sPr.driveLog;
           uint32_t* hist = sPr.hist;
           const uint32_t* refBall = sPr.refBall;
-          uint32_t* biasG = sNet.d.bias;
           for (uint32_t i = 0; i < cpw; ++i) {
             const uint32_t cc = gw + i * nwS;
             if (cc >= ncol) break;
