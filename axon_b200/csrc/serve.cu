@@ -5,7 +5,7 @@
 // any tick, so each carries its own local step: it reads spk(t-1) from its slot (all zero
 // at t = 0) and writes spk(t) into the other half of its ping-pong pair.
 //
-// k_serve_drive: a warp takes one (group of up to 8 trajectories of one network, column)
+// k_serve_drive: a warp takes one (group of up to kServeGroup trajectories of one network, column)
 // item. It loads each W3 tile that any member needs once and applies it to every member
 // whose presynaptic group is active, so the weights are read once per column per group
 // instead of once per trajectory; it writes each member's per-neuron drives and column drive.
@@ -27,7 +27,7 @@ constexpr uint32_t kEmitChunk = 256;   // gated columns whose per-neuron drives 
 
 // Spike vectors and activity bits were written by the previous tick's emit kernel and are
 // read-only here, so they are read through the non-coherent L1 path.
-__global__ void __launch_bounds__(kServeThreads, 3) k_serve_drive(ServeDev d, ServeCfg c) {
+__global__ void __launch_bounds__(kServeThreads, 4) k_serve_drive(ServeDev d, ServeCfg c) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t ncol = c.ncol, ngroups = d.counts[1];

@@ -6,7 +6,7 @@
 //             memory for all of the network's trajectories, lanes over (branch,
 //             trajectory) entries of nonzero spike words) or, for a network with few
 //             trajectories this tick, k_serve_drive (warps over columns, tiles shared by
-//             groups of 8 trajectories); both leave per-neuron and column drives in the slot;
+//             groups of kServeGroup trajectories); both leave per-neuron and column drives in the slot;
 //   emit      k_serve_emit: threshold select, exact k-of-32 for the gated columns, the
 //             spike vector, group-activity bits, and the entry lists of the next tick.
 #pragma once
@@ -16,7 +16,7 @@
 
 namespace axon {
 
-constexpr uint32_t kServeGroup = 8;      // trajectories of one network sharing a tile load (gather kernel)
+constexpr uint32_t kServeGroup = 2;      // trajectories of one network sharing a tile load (gather kernel)
 constexpr uint32_t kServeMaxB = 512;     // trajectories of one network per tick (list capacity)
 constexpr uint32_t kServeMaxB32 = 300;   // the same when drives are kept as u32 (shared-memory bound)
 constexpr uint32_t kServeBatchMin = 24;  // fewer trajectories of a network in a tick: gather kernel
