@@ -116,7 +116,14 @@ __global__ void __launch_bounds__(kEmitThreads) k_serve_emit(ServeDev d, ServeCf
   uint32_t* sCnt = sAccS + kEmitChunk * 32u;       // [0] gated columns
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
   const uint32_t nent = d.counts[0];
-  for (uint32_t ei = blockIdx.x; ei < nent; ei += gridDim.x) {
+  // work units: (trajectory, part). Every part selects the threshold over all drives; then
+  // it handles the columns of its own range, a multiple of 256 columns (whole groups and
+  // whole activity words), so the parts of a trajectory write disjoint data.
+  const uint32_t P = max(d.emitParts, 1u);
+  const uint32_t span = ((ncol + P * 256u - 1u) / (P * 256u)) * 256u;
+  for (uint32_t u = blockIdx.x; u < nent * P; u += gridDim.x) {
+    const uint32_t ei = u / P, part = u - ei * P;
+    const uint32_t c0 = min(part * span, ncol), c1 = min(c0 + span, ncol);
     const ServeEntry e = d.ent[ei];
     uint32_t* base = d.slots + (size_t)e.slot * d.slotWords;
     const uint32_t* xdrive = base + 2u * ncol + 2u * d.nactw;
@@ -139,7 +146,7 @@ __global__ void __launch_bounds__(kEmitThreads) k_serve_emit(ServeDev d, ServeCf
     const uint32_t gate = max(theta, 1u);
     // k_emit's gate and clamp (src/axon.mm:211-212): clamped input columns take the cue,
     // other columns spike only when their drive reaches the gate
-    for (uint32_t cc = tid; cc < ncol; cc += blockDim.x) {
+    for (uint32_t cc = c0 + tid; cc < c1; cc += blockDim.x) {
       uint32_t v = 0u;
       if (clamp && cc < incols) v = sStim[cc];
       else if (sD[cc] >= gate) sList[atomicAdd(sCnt, 1u)] = cc;
@@ -172,7 +179,7 @@ __global__ void __launch_bounds__(kEmitThreads) k_serve_emit(ServeDev d, ServeCf
     uint32_t* spkOut = base + (e.tloc & 1u) * ncol;
     uint32_t* actOut = base + 2u * ncol + (e.tloc & 1u) * d.nactw;
     uint4* dst = e.done != 0xFFFFFFFFu ? reinterpret_cast<uint4*>(d.doneBuf + (size_t)e.done * ncol) : nullptr;
-    for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x) {
+    for (uint32_t i = c0 / 4u + tid; i < c1 / 4u; i += blockDim.x) {
       const uint4 v = reinterpret_cast<const uint4*>(sSpk)[i];
       __stcg(reinterpret_cast<uint4*>(spkOut) + i, v);
       if (dst) dst[i] = v;
@@ -184,7 +191,7 @@ __global__ void __launch_bounds__(kEmitThreads) k_serve_emit(ServeDev d, ServeCf
       uint4* eMOut = net.entM + (size_t)q * ngrp * kServeMaxB;
       uint32_t* c1Out = net.ecnt + (size_t)q * 2 * ngrp;
       uint32_t* cMOut = c1Out + ngrp;
-      for (uint32_t g = tid; g < ngrp; g += blockDim.x) {
+      for (uint32_t g = c0 / 8u + tid; g < c1 / 8u; g += blockDim.x) {
         const uint4 p = reinterpret_cast<const uint4*>(sSpk)[2 * g], q4 = reinterpret_cast<const uint4*>(sSpk)[2 * g + 1];
         const uint32_t w[8] = {p.x, p.y, p.z, p.w, q4.x, q4.y, q4.z, q4.w};
         uint32_t nz = 0, S0 = 0u, S1 = 0u, S2 = 0u, k = 0, w0 = 0;
@@ -206,10 +213,10 @@ __global__ void __launch_bounds__(kEmitThreads) k_serve_emit(ServeDev d, ServeCf
         }
       }
     }
-    for (uint32_t gb = warp * 32u; gb < ngrp; gb += nw * 32u) {  // group-activity bits
+    for (uint32_t gb = c0 / 8u + warp * 32u; gb < c1 / 8u; gb += nw * 32u) {  // group-activity bits
       const uint32_t g = gb + lane;
       bool any = false;
-      if (g < ngrp) {
+      if (g < c1 / 8u) {
         const uint4 p = reinterpret_cast<const uint4*>(sSpk)[2 * g], q = reinterpret_cast<const uint4*>(sSpk)[2 * g + 1];
         any = (p.x | p.y | p.z | p.w | q.x | q.y | q.z | q.w) != 0u;
       }

@@ -67,7 +67,7 @@ struct ServeDev {
   uint32_t* doneBuf;         // [done][ncol] final spikes of trajectories that end this tick
   uint32_t slotWords, nactw;
   uint32_t par;              // tick parity: entry lists are read at par and written at par ^ 1
-  uint32_t pad;
+  uint32_t emitParts;        // CTAs sharing one trajectory's emit, each on its own column range
   uint64_t waitNs;           // bound on the batched kernel's copy waits
   uint32_t* err;             // device error word
 };

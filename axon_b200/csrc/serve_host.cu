@@ -338,6 +338,8 @@ axon_status axon_server::tick() {
   td.btab = (const uint2*)(ds + oTab);
   td.cues = (const uint32_t*)(ds + oCue);
   td.par = par;
+  // few trajectories: several CTAs share each one's emit (the grid has sms * 2 CTAs)
+  td.emitParts = ne * 4u <= (uint32_t)sms * 2u ? 4u : (ne * 2u <= (uint32_t)sms * 2u ? 2u : 1u);
   CKS(cudaMemcpyAsync(ds, h, bytes, cudaMemcpyHostToDevice, stream));
   const uint32_t eb = pendingEv ^ 1u;  // this tick's events (the previous tick's are still to be read)
   CKS(cudaEventRecord(ev[eb][0], stream));
