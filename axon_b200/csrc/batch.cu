@@ -52,10 +52,10 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   constexpr uint32_t accStride = PACK ? 17u : 33u;  // padded: distinct trajectories hit distinct banks
   uint32_t* sTile = sm;                                  // [2][kItemWords]
   uint32_t* sAcc = sTile + 2 * kItemWords;               // [kRecallCpi][B][accStride]
-  uint32_t* sConn = sAcc + kRecallCpi * B * accStride;   // [64]
-  uint32_t* sP1 = sConn + 64;                            // [68] single-word entries: prefix over 64 branches
-  uint32_t* sPM = sP1 + 68;                              // [68] multi-word entries
-  uint32_t* sMisc = sPM + 68;                            // [16]
+  uint32_t* sConn = sAcc + kRecallCpi * B * accStride;   // [2][64] groups of the item's branches
+  uint32_t* sP1 = sConn + 2 * 64;                        // [2][68] single-word entries: prefix over 64 branches
+  uint32_t* sPM = sP1 + 2 * 68;                          // [2][68] multi-word entries
+  uint32_t* sMisc = sPM + 2 * 68;                        // [16]
   uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
   // phase-2 views reuse the tile buffers
   uint32_t* sD = sTile;
@@ -83,6 +83,29 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     mbar_expect_tx(&sBar[buf], ncols * kColWords * 4u);
     for (uint32_t k = 0; k < ncols; ++k)
       bulk_g2s(sTile + buf * kItemWords + k * kColWords, d.W3R + (size_t)(c0 + k) * kColWords, kColWords * 4u, &sBar[buf]);
+  };
+  // warps 0 and 1: the item's branch groups and the prefixes of its 64 entry-list lengths,
+  // single-word (warp 0) and multi-word (warp 1), into buffer buf
+  auto prep = [&](uint32_t item, uint32_t buf, const uint32_t* c1In, const uint32_t* cMIn) {
+    const uint32_t c0 = item * kRecallCpi;
+    const bool v1 = c0 + 1 < ncol;
+    const uint32_t g0 = __ldg(d.conn + c0 * kNslot + lane), g1 = v1 ? __ldg(d.conn + (c0 + 1) * kNslot + lane) : 0u;
+    if (warp == 0) {
+      sConn[buf * 64u + lane] = g0;
+      sConn[buf * 64u + 32u + lane] = g1;
+    }
+    const uint32_t* cin = warp ? cMIn : c1In;
+    uint32_t* P = (warp ? sPM : sP1) + buf * 68u;
+    uint32_t i0 = __ldcg(cin + g0), i1 = v1 ? __ldcg(cin + g1) : 0u;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t a = __shfl_up_sync(kFull, i0, off), b = __shfl_up_sync(kFull, i1, off);
+      if (lane >= (uint32_t)off) { i0 += a; i1 += b; }
+    }
+    const uint32_t tot0 = __shfl_sync(kFull, i0, 31);
+    P[1 + lane] = i0;
+    P[33 + lane] = tot0 + i1;
+    if (lane == 0) P[0] = 0u;
   };
 
   for (uint32_t t = 0; t < c.T; ++t) {
@@ -116,6 +139,8 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     }
     __syncthreads();
     uint32_t item = sMisc[1];
+    if (warp < 2 && item < nitems) prep(item, kbuf, c1In, cMIn);
+    __syncthreads();
     while (item < nitems) {
       const uint32_t bcur = kbuf;
       if (tid == 0) {
@@ -128,28 +153,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         }
       }
       const uint32_t c0 = item * kRecallCpi;
-      for (uint32_t i = tid; i < 64u; i += blockDim.x) {
-        const uint32_t col = c0 + (i >> 5);
-        sConn[i] = col < ncol ? __ldg(d.conn + col * kNslot + (i & 31u)) : 0u;
-      }
       for (uint32_t i = tid; i < kRecallCpi * B * accStride; i += blockDim.x) sAcc[i] = 0u;
-      __syncthreads();
-      if (warp < 2) {  // prefixes of the 64 list lengths, single-word (warp 0) and multi-word (warp 1)
-        const uint32_t* cin = warp ? cMIn : c1In;
-        uint32_t* P = warp ? sPM : sP1;
-        const bool v1 = c0 + 1 < ncol;
-        const uint32_t n0 = __ldcg(cin + sConn[lane]), n1 = v1 ? __ldcg(cin + sConn[32 + lane]) : 0u;
-        uint32_t i0 = n0, i1 = n1;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-          const uint32_t a = __shfl_up_sync(kFull, i0, off), b = __shfl_up_sync(kFull, i1, off);
-          if (lane >= (uint32_t)off) { i0 += a; i1 += b; }
-        }
-        const uint32_t tot0 = __shfl_sync(kFull, i0, 31);
-        P[1 + lane] = i0;
-        P[33 + lane] = tot0 + i1;
-        if (lane == 0) P[0] = 0u;
-      }
       const uint32_t parCur = (bcur ? uses1 : uses0) & 1u;
       const bool ok = mbar_wait(&sBar[bcur], parCur, c.waitNs);
       if (bcur) ++uses1; else ++uses0;
@@ -165,7 +169,14 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         __syncthreads();
         return;
       }
-      const uint32_t E1 = sP1[64], E = E1 + sPM[64], units = (E + 31u) >> 5;
+      // the next item's groups and prefixes load while this item computes (warps 0 and 1
+      // join the entry units late; the units are claimed dynamically)
+      const uint32_t next = sMisc[2];
+      if (warp < 2 && next < nitems) prep(next, bcur ^ 1u, c1In, cMIn);
+      const uint32_t* cConn = sConn + bcur * 64u;
+      const uint32_t* cP1 = sP1 + bcur * 68u;
+      const uint32_t* cPM = sPM + bcur * 68u;
+      const uint32_t E1 = cP1[64], E = E1 + cPM[64], units = (E + 31u) >> 5;
       const uint32_t* tileBase = sTile + bcur * kItemWords;
       for (;;) {
         uint32_t u = 0;
@@ -175,14 +186,14 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         uint32_t flat = u * 32u + lane;
         if (flat >= E) continue;
         const bool single = flat < E1;
-        const uint32_t* P = single ? sP1 : sPM;
+        const uint32_t* P = single ? cP1 : cPM;
         if (!single) flat -= E1;
         uint32_t sp = 0;
 #pragma unroll
         for (uint32_t step = 32; step; step >>= 1)
           if (sp + step < 64u && P[sp + step] <= flat) sp += step;
         const uint32_t e = flat - P[sp];
-        const uint32_t g = sConn[sp];
+        const uint32_t g = cConn[sp];
         const uint32_t* tile = tileBase + (sp >> 5) * kColWords + (sp & 31u) * 256u;
         if (single) {  // one nonzero word: 32 AND-counts
           const uint2 en = __ldcg(e1In + (size_t)g * B + e);
@@ -270,7 +281,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         }
       }
       __syncthreads();
-      item = sMisc[2];
+      item = next;
       kbuf ^= 1u;
     }
     if (!grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;
@@ -358,7 +369,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
 size_t recall_smem_bytes(uint32_t ncol, uint32_t B, uint32_t acc32) {
   (void)ncol;
   const size_t stride = acc32 ? 33 : 17;
-  return (2ull * kItemWords + kRecallCpi * (size_t)B * stride + 64 + 68 + 68 + 16 + 4) * 4;
+  return (2ull * kItemWords + kRecallCpi * (size_t)B * stride + 2 * (64 + 68 + 68) + 16 + 4) * 4;
 }
 
 namespace {
