@@ -71,6 +71,8 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     mbar_init(&sBar[1], 1);
     fence_proxy_async_smem();
   }
+  // the counters start at zero; each item's write-back clears what it read
+  for (uint32_t i = tid; i < kRecallCpi * B * accStride; i += blockDim.x) sAcc[i] = 0u;
   __syncthreads();
   uint32_t uses0 = 0, uses1 = 0;  // completed phases per buffer
   uint32_t kbuf = 0;              // buffer of the next item
@@ -153,7 +155,6 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         }
       }
       const uint32_t c0 = item * kRecallCpi;
-      for (uint32_t i = tid; i < kRecallCpi * B * accStride; i += blockDim.x) sAcc[i] = 0u;
       const uint32_t parCur = (bcur ? uses1 : uses0) & 1u;
       const bool ok = mbar_wait(&sBar[bcur], parCur, c.waitNs);
       if (bcur) ++uses1; else ++uses0;
@@ -242,8 +243,9 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         for (uint32_t pp = warp * 8u + grp; pp < kRecallCpi * B; pp += nw * 8u) {
           const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
           if (col >= ncol) continue;  // uniform over the four lanes
-          const uint32_t* src = sAcc + (colL * B + b) * accStride + q * 4u;
+          uint32_t* src = sAcc + (colL * B + b) * accStride + q * 4u;
           const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
+          src[0] = src[1] = src[2] = src[3] = 0u;
           reinterpret_cast<uint4*>(d.acc)[(((size_t)b * ncol + col) * 16u >> 2) + q] = w;
           uint32_t s = (w.x & 0xFFFFu) + (w.x >> 16) + (w.y & 0xFFFFu) + (w.y >> 16) + (w.z & 0xFFFFu) + (w.z >> 16) +
                        (w.w & 0xFFFFu) + (w.w >> 16);
@@ -255,8 +257,10 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         for (uint32_t pp = warp; pp < kRecallCpi * B; pp += nw) {
           const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
           if (col >= ncol) continue;
-          const uint32_t* ab = sAcc + (colL * B + b) * accStride;
+          uint32_t* ab = sAcc + (colL * B + b) * accStride;
           uint32_t a = PACK ? ((ab[lane >> 1] >> (16u * (lane & 1u))) & 0xFFFFu) : ab[lane];
+          __syncwarp();
+          if (lane < (PACK ? 16u : 32u)) ab[lane] = 0u;
           if (c.facil != 0u && ((__ldcg(spkIn + (size_t)b * ncol + col) >> lane) & 1u)) a += c.facil;
           const uint32_t biasL = c.useBias ? (__ldg(d.bias + col * 32u + lane) >> c.biasShift) : 0u;
           a = a > biasL ? a - biasL : 0u;
@@ -280,7 +284,8 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
           }
         }
       }
-      __syncthreads();
+      // no barrier here: the next item's first shared-memory writes (counter atomics, the
+      // prefixes of the item after it) come after the next __syncthreads_or
       item = next;
       kbuf ^= 1u;
     }

@@ -35,10 +35,10 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
   constexpr uint32_t maxB = sb_maxb<PACK>();
   uint32_t* sTile = sm;                                     // [2][kItemWords]
   uint32_t* sAcc = sTile + 2 * kItemWords;                  // [kRecallCpi][B][accStride]
-  uint32_t* sConn = sAcc + kRecallCpi * maxB * accStride;   // [64]
-  uint32_t* sP1 = sConn + 64;                               // [68] single-word entries: prefix over 64 branches
-  uint32_t* sPM = sP1 + 68;                                 // [68] multi-word entries
-  uint32_t* sMisc = sPM + 68;                               // [16]
+  uint32_t* sConn = sAcc + kRecallCpi * maxB * accStride;   // [2][64] groups of the item's branches
+  uint32_t* sP1 = sConn + 2 * 64;                           // [2][68] single-word entries: prefix over 64 branches
+  uint32_t* sPM = sP1 + 2 * 68;                             // [2][68] multi-word entries
+  uint32_t* sMisc = sPM + 2 * 68;                           // [16]
   uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
   const uint32_t nip = (ncol + kRecallCpi - 1) / kRecallCpi;  // work items per network
@@ -49,6 +49,8 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
     mbar_init(&sBar[1], 1);
     fence_proxy_async_smem();
   }
+  // the counters start at zero; each item's write-back clears what it read
+  for (uint32_t i = tid; i < kRecallCpi * maxB * accStride; i += blockDim.x) sAcc[i] = 0u;
   __syncthreads();
   uint32_t uses0 = 0, uses1 = 0, kbuf = 0;
 
@@ -60,6 +62,32 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
     mbar_expect_tx(&sBar[buf], ncols * kColWords * 4u);
     for (uint32_t k = 0; k < ncols; ++k)
       bulk_g2s(sTile + buf * kItemWords + k * kColWords, W3R + (size_t)(c0 + k) * kColWords, kColWords * 4u, &sBar[buf]);
+  };
+  // warps 0 and 1: the item's branch groups and the prefixes of its 64 entry-list lengths,
+  // single-word (warp 0) and multi-word (warp 1), into buffer buf
+  auto prep = [&](uint32_t it, uint32_t buf) {
+    const ServeBNet pn = d.bnets[it / nip];
+    const uint32_t* conn = d.nets[pn.net].conn;
+    const uint32_t* c1 = d.nets[pn.net].ecnt + (size_t)d.par * 2 * ngrp;
+    const uint32_t c0 = (it % nip) * kRecallCpi;
+    const bool v1 = c0 + 1 < ncol;
+    const uint32_t g0 = __ldg(conn + c0 * kNslot + lane), g1 = v1 ? __ldg(conn + (c0 + 1) * kNslot + lane) : 0u;
+    if (warp == 0) {
+      sConn[buf * 64u + lane] = g0;
+      sConn[buf * 64u + 32u + lane] = g1;
+    }
+    const uint32_t* cin = warp ? c1 + ngrp : c1;
+    uint32_t* P = (warp ? sPM : sP1) + buf * 68u;
+    uint32_t i0 = __ldcg(cin + g0), i1 = v1 ? __ldcg(cin + g1) : 0u;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t a = __shfl_up_sync(kFull, i0, off), b = __shfl_up_sync(kFull, i1, off);
+      if (lane >= (uint32_t)off) { i0 += a; i1 += b; }
+    }
+    const uint32_t tot0 = __shfl_sync(kFull, i0, 31);
+    P[1 + lane] = i0;
+    P[33 + lane] = tot0 + i1;
+    if (lane == 0) P[0] = 0u;
   };
   auto spk_prev = [&](uint32_t tabOff, uint32_t b) -> const uint32_t* {  // spk(t-1) of batch index b
     const uint2 st = __ldg(d.btab + tabOff + b);
@@ -78,6 +106,8 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
   }
   __syncthreads();
   uint32_t item = sMisc[1];
+  if (warp < 2 && item < nitems) prep(item, kbuf);
+  __syncthreads();
   while (item < nitems) {
     const uint32_t bcur = kbuf;
     if (tid == 0) {
@@ -90,35 +120,10 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
       }
     }
     const ServeBNet bn = d.bnets[item / nip];
-    const uint32_t* conn = d.nets[bn.net].conn;
     const uint2* e1In = d.nets[bn.net].ent1 + (size_t)d.par * ngrp * kServeMaxB;
     const uint4* eMIn = d.nets[bn.net].entM + (size_t)d.par * ngrp * kServeMaxB;
-    const uint32_t* c1In = d.nets[bn.net].ecnt + (size_t)d.par * 2 * ngrp;
-    const uint32_t* cMIn = c1In + ngrp;
     const uint32_t B = bn.B;
     const uint32_t c0 = (item % nip) * kRecallCpi;
-    for (uint32_t i = tid; i < 64u; i += blockDim.x) {
-      const uint32_t col = c0 + (i >> 5);
-      sConn[i] = col < ncol ? __ldg(conn + col * kNslot + (i & 31u)) : 0u;
-    }
-    for (uint32_t i = tid; i < kRecallCpi * B * accStride; i += blockDim.x) sAcc[i] = 0u;
-    __syncthreads();
-    if (warp < 2) {  // prefixes of the 64 list lengths, single-word (warp 0) and multi-word (warp 1)
-      const uint32_t* cin = warp ? cMIn : c1In;
-      uint32_t* P = warp ? sPM : sP1;
-      const bool v1 = c0 + 1 < ncol;
-      const uint32_t n0 = __ldcg(cin + sConn[lane]), n1 = v1 ? __ldcg(cin + sConn[32 + lane]) : 0u;
-      uint32_t i0 = n0, i1 = n1;
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const uint32_t a = __shfl_up_sync(kFull, i0, off), b = __shfl_up_sync(kFull, i1, off);
-        if (lane >= (uint32_t)off) { i0 += a; i1 += b; }
-      }
-      const uint32_t tot0 = __shfl_sync(kFull, i0, 31);
-      P[1 + lane] = i0;
-      P[33 + lane] = tot0 + i1;
-      if (lane == 0) P[0] = 0u;
-    }
     const uint32_t parCur = (bcur ? uses1 : uses0) & 1u;
     const bool ok = mbar_wait(&sBar[bcur], parCur, d.waitNs);
     if (bcur) ++uses1; else ++uses0;
@@ -133,7 +138,14 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
       __syncthreads();
       return;
     }
-    const uint32_t E1 = sP1[64], E = E1 + sPM[64], units = (E + 31u) >> 5;
+    // the next item's groups and prefixes load while this item computes (warps 0 and 1
+    // join the entry units late; the units are claimed dynamically)
+    const uint32_t next = sMisc[2];
+    if (warp < 2 && next < nitems) prep(next, bcur ^ 1u);
+    const uint32_t* cConn = sConn + bcur * 64u;
+    const uint32_t* cP1 = sP1 + bcur * 68u;
+    const uint32_t* cPM = sPM + bcur * 68u;
+    const uint32_t E1 = cP1[64], E = E1 + cPM[64], units = (E + 31u) >> 5;
     const uint32_t* tileBase = sTile + bcur * kItemWords;
     for (;;) {
       uint32_t u = 0;
@@ -143,14 +155,14 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
       uint32_t flat = u * 32u + lane;
       if (flat >= E) continue;
       const bool single = flat < E1;
-      const uint32_t* P = single ? sP1 : sPM;
+      const uint32_t* P = single ? cP1 : cPM;
       if (!single) flat -= E1;
       uint32_t sp = 0;
 #pragma unroll
       for (uint32_t step = 32; step; step >>= 1)
         if (sp + step < 64u && P[sp + step] <= flat) sp += step;
       const uint32_t e = flat - P[sp];
-      const uint32_t g = sConn[sp];
+      const uint32_t g = cConn[sp];
       const uint32_t* tile = tileBase + (sp >> 5) * kColWords + (sp & 31u) * 256u;
       if (single) {  // one nonzero word: 32 AND-counts
         const uint2 en = __ldcg(e1In + (size_t)g * kServeMaxB + e);
@@ -200,8 +212,9 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
         const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
         if (col >= ncol) continue;  // uniform over the four lanes
         uint32_t* base = d.slots + (size_t)__ldg(d.btab + bn.tabOff + b).x * d.slotWords;
-        const uint32_t* src = sAcc + (colL * B + b) * accStride + q * 4u;
+        uint32_t* src = sAcc + (colL * B + b) * accStride + q * 4u;
         const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
+        src[0] = src[1] = src[2] = src[3] = 0u;
         __stcg(reinterpret_cast<uint4*>(base + accOff + col * 16u) + q, w);
         uint32_t s = (w.x & 0xFFFFu) + (w.x >> 16) + (w.y & 0xFFFFu) + (w.y >> 16) + (w.z & 0xFFFFu) + (w.z >> 16) +
                      (w.w & 0xFFFFu) + (w.w >> 16);
@@ -216,6 +229,7 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
         const uint2 st = __ldg(d.btab + bn.tabOff + b);
         uint32_t* base = d.slots + (size_t)st.x * d.slotWords;
         uint32_t a = sAcc[(colL * B + b) * accStride + lane];
+        sAcc[(colL * B + b) * accStride + lane] = 0u;  // one lane per word
         if (c.facil != 0u && st.y > 0u && ((__ldcg(base + ((st.y - 1u) & 1u) * ncol + col) >> lane) & 1u)) a += c.facil;
         if (c.acc32) __stcg(base + accOff + col * 32u + lane, a);
         else __stcg(reinterpret_cast<unsigned short*>(base + accOff) + col * 32u + lane, (unsigned short)a);
@@ -223,15 +237,16 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
         if (lane == 0) __stcg(base + xOff + col, dsum);
       }
     }
-    __syncthreads();
-    item = sMisc[2];
+    // no barrier here: the next item's first shared-memory writes (counter atomics, the
+    // prefixes of the item after it) come after the next __syncthreads_or
+    item = next;
     kbuf ^= 1u;
   }
 }
 
 size_t serve_batched_smem_bytes(uint32_t packed) {
   const size_t maxB = packed ? kServeMaxB : kServeMaxB32, stride = packed ? 17 : 33;
-  return (2ull * kItemWords + kRecallCpi * maxB * stride + 64 + 68 + 68 + 16 + 4) * 4;
+  return (2ull * kItemWords + kRecallCpi * maxB * stride + 2 * (64 + 68 + 68) + 16 + 4) * 4;
 }
 
 namespace {
