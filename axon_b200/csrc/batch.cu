@@ -57,8 +57,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   uint32_t* sPM = sP1 + 2 * 68;                          // [2][68] multi-word entries
   uint32_t* sMisc = sPM + 2 * 68;                        // [16]
   uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
-  // phase-2 views reuse the tile buffers
-  uint32_t* sD = sTile;
+  // phase-2 views reuse the tile buffers; a second drive buffer follows them when it fits
   uint32_t* sSpk = sTile + ncol;
   uint32_t* sList = sTile + 2 * ncol;
   uint32_t* sRed = sTile + 3 * ncol;  // 192 words
@@ -292,10 +291,23 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     if (!grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;
 
     // ---------------- phase 2: threshold, gated k-of-32 ballots, next spike vectors and lists
-    for (uint32_t b = blockIdx.x; b < B; b += gridDim.x) {
-      const uint32_t* drvb = d.drv + (size_t)b * ncol;
-      for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x)
-        reinterpret_cast<uint4*>(sD)[i] = __ldcg(reinterpret_cast<const uint4*>(drvb) + i);
+    // The column drives of the CTA's trajectories arrive by asynchronous copies; with two
+    // buffers the next trajectory's copy is in flight while the current one is processed.
+    const bool dbuf = 4u * ncol + 448u <= 2u * kItemWords;
+    uint32_t* const sDalt = sTile + 3u * ncol + 448u;
+    auto load_drv = [&](uint32_t b, uint32_t* dst) {
+      const uint4* src = reinterpret_cast<const uint4*>(d.drv + (size_t)b * ncol);
+      for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x) cp_async16(reinterpret_cast<uint4*>(dst) + i, src + i);
+    };
+    if (blockIdx.x < B) load_drv(blockIdx.x, sTile);
+    cp_async_commit();
+    for (uint32_t b = blockIdx.x, k = 0; b < B; b += gridDim.x, ++k) {
+      uint32_t* sD = (dbuf && (k & 1u)) ? sDalt : sTile;
+      const uint32_t bNext = b + gridDim.x;
+      if (dbuf && bNext < B) load_drv(bNext, (k & 1u) ? sTile : sDalt);
+      cp_async_commit();
+      if (dbuf) cp_async_wait<1>();  // all but the copy just issued: this trajectory's drives
+      else cp_async_wait<0>();
       if (tid == 0) sMisc[4] = 0u;
       __syncthreads();
       const uint32_t theta = block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed, __ldcg(d.thPrev + b));
@@ -309,24 +321,41 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       }
       __syncthreads();
       const uint32_t npend = sMisc[4];
-      for (uint32_t e = warp; e < npend; e += nw) {
-        const uint32_t cc = sList[e];
-        const uint32_t a = c.acc32 ? __ldcg(reinterpret_cast<const uint32_t*>(d.acc) + ((size_t)b * ncol + cc) * 32u + lane)
-                                   : (uint32_t)__ldcg(reinterpret_cast<const uint16_t*>(d.acc) + ((size_t)b * ncol + cc) * 32u + lane);
-        uint32_t vk, vk1;
-        const uint32_t ball = warp_kwta(a, lane, c.k, vk, vk1);
-        if (lane == 0) {
-          sSpk[cc] = ball;
-          if (d.stats && ball != 0u && cc >= incols) {  // k_emit counters, src/axon.mm:225-234
-            uint32_t* st = d.stats + (size_t)b * 1024u;
-            const uint32_t sb = 64u + t * 8u;
-            atomicAdd(st + 0, 1u);
-            atomicAdd(st + 1, (uint32_t)__popc(ball));
-            atomicAdd(st + sb + 0u, vk - vk1);
-            atomicAdd(st + sb + 1u, vk);
-            atomicAdd(st + sb + 2u, 1u);
-            if (vk == vk1) atomicAdd(st + sb + 3u, 1u);
-            if (vk == 0u) atomicAdd(st + sb + 4u, 1u);
+      // a warp's gated columns kPend at a time: their per-neuron drives load together
+      constexpr uint32_t kPend = 4;
+      for (uint32_t e0 = warp; e0 < npend; e0 += kPend * nw) {
+        uint32_t av[kPend];
+#pragma unroll
+        for (uint32_t u = 0; u < kPend; ++u) {
+          const uint32_t e = e0 + u * nw;
+          av[u] = 0u;
+          if (e < npend) {
+            const size_t o = ((size_t)b * ncol + sList[e]) * 32u + lane;
+            av[u] = c.acc32 ? __ldcg(reinterpret_cast<const uint32_t*>(d.acc) + o)
+                            : (uint32_t)__ldcg(reinterpret_cast<const uint16_t*>(d.acc) + o);
+          }
+        }
+#pragma unroll
+        for (uint32_t u = 0; u < kPend; ++u) {
+          const uint32_t e = e0 + u * nw;
+          if (e >= npend) break;  // warp-uniform
+          const uint32_t cc = sList[e];
+          const uint32_t a = av[u];
+          uint32_t vk, vk1;
+          const uint32_t ball = warp_kwta(a, lane, c.k, vk, vk1);
+          if (lane == 0) {
+            sSpk[cc] = ball;
+            if (d.stats && ball != 0u && cc >= incols) {  // k_emit counters, src/axon.mm:225-234
+              uint32_t* st = d.stats + (size_t)b * 1024u;
+              const uint32_t sb = 64u + t * 8u;
+              atomicAdd(st + 0, 1u);
+              atomicAdd(st + 1, (uint32_t)__popc(ball));
+              atomicAdd(st + sb + 0u, vk - vk1);
+              atomicAdd(st + sb + 1u, vk);
+              atomicAdd(st + sb + 2u, 1u);
+              if (vk == vk1) atomicAdd(st + sb + 3u, 1u);
+              if (vk == 0u) atomicAdd(st + sb + 4u, 1u);
+            }
           }
         }
       }
@@ -366,7 +395,9 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         if (d.theta && t + 1u == c.T) d.theta[b] = theta;
       }
       __syncthreads();
+      if (!dbuf && bNext < B) load_drv(bNext, sTile);  // committed at the next trajectory's start
     }
+    cp_async_wait<0>();
     if (t + 1u < c.T && !grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;
   }
 }

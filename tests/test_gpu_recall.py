@@ -98,10 +98,34 @@ def test_recall_batched_equals_plain_full_geometry():
     assert np.array_equal(rb["hist"][idx], h)
 
 
+@pytest.mark.parametrize("B", [149, 320])
+def test_recall_several_trajectories_per_cta(B):
+    """More trajectories than CTAs (one per SM, 148 on a B200): a CTA selects the
+    thresholds of two or three trajectories in turn, the next one's drives loading while
+    the current one is processed. Every trajectory equals the plain method; a sample,
+    including trajectories of a CTA's second and third turn, equals the oracle."""
+    cfg, gpu, cpu, pats = trained_pair({}, 6, 3, 16)
+    cues = make_cues(pats, cfg.ncol, B, np.random.default_rng(B))
+    rb = gpu.recall(cues, 20, 5, hist=True, stats=True)
+    rp = gpu.recall(cues, 20, 5, hist=True, method="plain")
+    assert np.array_equal(rb["final"], rp["final"])
+    assert np.array_equal(rb["hist"], rp["hist"])
+    idx = [0, 148, B - 1]
+    f, h, s, _ = oracle_runs(cpu, cues[idx], 20, 5, 0)
+    assert np.array_equal(rb["final"][idx], f)
+    assert np.array_equal(rb["hist"][idx], h)
+    s = s.copy()
+    s[:, 2] = 0  # branch coincidence: plain method only
+    st = rb["stats"][idx].copy()
+    st[:, 2] = 0
+    assert np.array_equal(st, s)
+
+
 def test_batched_equals_plain_at_the_widest_batched_network():
     """ncol = 8,192, the widest network the batched kernel takes (the plain path at that
     width is checked against the oracle in test_gpu_plain): both methods agree on every
-    trajectory's spikes at every step."""
+    trajectory's spikes at every step. 160 trajectories put two on some CTAs; at this
+    width the threshold step has room for one drive buffer only."""
     import axon_b200 as ax
 
     cfg = ax.config(ncol=8192, incols=512, **ax.CONFIG_C)
@@ -110,7 +134,7 @@ def test_batched_equals_plain_at_the_widest_batched_network():
         pats = ax.stimuli(4, 6, 512, 64)
         for p in range(6):
             net.present(ax.load_stim(pats[p], 1.0, 1000 + p, 8192), 10, 5, True)
-        cues = np.stack([ax.load_stim(pats[q % 6], 0.6 + 0.05 * (q % 5), 4400 + q, 8192) for q in range(20)])
+        cues = np.stack([ax.load_stim(pats[q % 6], 0.6 + 0.05 * (q % 5), 4400 + q, 8192) for q in range(160)])
         a = net.recall(cues, 25, 6, hist=True)
         b = net.recall(cues, 25, 6, hist=True, method="plain")
         assert np.array_equal(a["hist"], b["hist"]) and np.array_equal(a["final"], b["final"])
