@@ -145,7 +145,9 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
     const uint32_t* cConn = sConn + bcur * 64u;
     const uint32_t* cP1 = sP1 + bcur * 68u;
     const uint32_t* cPM = sPM + bcur * 68u;
-    const uint32_t E1 = cP1[64], E = E1 + cPM[64], units = (E + 31u) >> 5;
+    // multi-word entries (the costlier ones) are dealt first, so the units that finish last
+    // are single-word ones
+    const uint32_t E1 = cP1[64], EM = cPM[64], E = E1 + EM, units = (E + 31u) >> 5;
     const uint32_t* tileBase = sTile + bcur * kItemWords;
     for (;;) {
       uint32_t u = 0;
@@ -154,9 +156,9 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
       if (u >= units) break;
       uint32_t flat = u * 32u + lane;
       if (flat >= E) continue;
-      const bool single = flat < E1;
+      const bool single = flat >= EM;
       const uint32_t* P = single ? cP1 : cPM;
-      if (!single) flat -= E1;
+      if (single) flat -= EM;
       uint32_t sp = 0;
 #pragma unroll
       for (uint32_t step = 32; step; step >>= 1)
@@ -168,7 +170,7 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
         const uint2 en = __ldcg(e1In + (size_t)g * kServeMaxB + e);
         const uint32_t b = en.x & 0xFFFFu, w = en.x >> 16, S = en.y;
         uint32_t* accb = sAcc + ((sp >> 5) * B + b) * accStride;
-#pragma unroll 4
+#pragma unroll
         for (uint32_t r = 0; r < 32u; r += 4) {
           const uint4 a = *reinterpret_cast<const uint4*>(tile + w3r_pos(r, w));
           acc_add4<PACK>(accb, r, branch_term<LIN>(__popc(a.x & S), dthr, bst),
