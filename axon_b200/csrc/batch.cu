@@ -51,11 +51,12 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   const uint32_t dthr = c.dthr, bst = c.bst;
   constexpr uint32_t accStride = PACK ? 17u : 33u;  // padded: distinct trajectories hit distinct banks
   uint32_t* sTile = sm;                                  // [2][kItemWords]
-  uint32_t* sAcc = sTile + 2 * kItemWords;               // [kRecallCpi][B][accStride]
-  uint32_t* sConn = sAcc + kRecallCpi * B * accStride;   // [2][64] groups of the item's branches
+  const uint32_t accWords = kRecallCpi * B * accStride;
+  uint32_t* sAcc = sTile + 2 * kItemWords;               // [1 or 2][kRecallCpi][B][accStride]
+  uint32_t* sConn = sAcc + (c.dacc ? 2u : 1u) * accWords;  // [2][64] groups of the item's branches
   uint32_t* sP1 = sConn + 2 * 64;                        // [2][68] single-word entries: prefix over 64 branches
   uint32_t* sPM = sP1 + 2 * 68;                          // [2][68] multi-word entries
-  uint32_t* sMisc = sPM + 2 * 68;                        // [16]
+  uint32_t* sMisc = sPM + 2 * 68;  // [16]: grid barrier flag, first item, -, -, gated count, -, unit counters [2], next items [2]
   uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
   // phase-2 views reuse the tile buffers; a second drive buffer follows them when it fits
   uint32_t* sSpk = sTile + ncol;
@@ -71,7 +72,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     fence_proxy_async_smem();
   }
   // the counters start at zero; each item's write-back clears what it read
-  for (uint32_t i = tid; i < kRecallCpi * B * accStride; i += blockDim.x) sAcc[i] = 0u;
+  for (uint32_t i = tid; i < (c.dacc ? 2u : 1u) * accWords; i += blockDim.x) sAcc[i] = 0u;
   __syncthreads();
   uint32_t uses0 = 0, uses1 = 0;  // completed phases per buffer
   uint32_t kbuf = 0;              // buffer of the next item
@@ -85,28 +86,30 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     for (uint32_t k = 0; k < ncols; ++k)
       bulk_g2s(sTile + buf * kItemWords + k * kColWords, d.W3R + (size_t)(c0 + k) * kColWords, kColWords * 4u, &sBar[buf]);
   };
-  // warps 0 and 1: the item's branch groups and the prefixes of its 64 entry-list lengths,
-  // single-word (warp 0) and multi-word (warp 1), into buffer buf
+  // warp 0: the item's branch groups and the prefixes of its 64 entry-list lengths, single-
+  // word and multi-word, into buffer buf
   auto prep = [&](uint32_t item, uint32_t buf, const uint32_t* c1In, const uint32_t* cMIn) {
     const uint32_t c0 = item * kRecallCpi;
     const bool v1 = c0 + 1 < ncol;
     const uint32_t g0 = __ldg(d.conn + c0 * kNslot + lane), g1 = v1 ? __ldg(d.conn + (c0 + 1) * kNslot + lane) : 0u;
-    if (warp == 0) {
-      sConn[buf * 64u + lane] = g0;
-      sConn[buf * 64u + 32u + lane] = g1;
-    }
-    const uint32_t* cin = warp ? cMIn : c1In;
-    uint32_t* P = (warp ? sPM : sP1) + buf * 68u;
-    uint32_t i0 = __ldcg(cin + g0), i1 = v1 ? __ldcg(cin + g1) : 0u;
+    sConn[buf * 64u + lane] = g0;
+    sConn[buf * 64u + 32u + lane] = g1;
+    uint32_t a0 = __ldcg(c1In + g0), a1 = v1 ? __ldcg(c1In + g1) : 0u;
+    uint32_t m0 = __ldcg(cMIn + g0), m1 = v1 ? __ldcg(cMIn + g1) : 0u;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-      const uint32_t a = __shfl_up_sync(kFull, i0, off), b = __shfl_up_sync(kFull, i1, off);
-      if (lane >= (uint32_t)off) { i0 += a; i1 += b; }
+      const uint32_t x0 = __shfl_up_sync(kFull, a0, off), x1 = __shfl_up_sync(kFull, a1, off);
+      const uint32_t y0 = __shfl_up_sync(kFull, m0, off), y1 = __shfl_up_sync(kFull, m1, off);
+      if (lane >= (uint32_t)off) { a0 += x0; a1 += x1; m0 += y0; m1 += y1; }
     }
-    const uint32_t tot0 = __shfl_sync(kFull, i0, 31);
-    P[1 + lane] = i0;
-    P[33 + lane] = tot0 + i1;
-    if (lane == 0) P[0] = 0u;
+    const uint32_t totA = __shfl_sync(kFull, a0, 31), totM = __shfl_sync(kFull, m0, 31);
+    uint32_t* P1 = sP1 + buf * 68u;
+    uint32_t* PM = sPM + buf * 68u;
+    P1[1 + lane] = a0;
+    P1[33 + lane] = totA + a1;
+    PM[1 + lane] = m0;
+    PM[33 + lane] = totM + m1;
+    if (lane == 0) P1[0] = PM[0] = 0u;
   };
 
   for (uint32_t t = 0; t < c.T; ++t) {
@@ -133,6 +136,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     if (tid == 0) {
       const uint32_t it0 = atomicAdd(d.work + t, 1u);
       sMisc[1] = it0;
+      sMisc[6] = sMisc[7] = 0u;
       if (it0 < nitems) {
         issue(it0, kbuf);
         claim = atomicAdd(d.work + t, 1u);
@@ -140,39 +144,38 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     }
     __syncthreads();
     uint32_t item = sMisc[1];
-    if (warp < 2 && item < nitems) prep(item, kbuf, c1In, cMIn);
+    if (warp == 0 && item < nitems) prep(item, kbuf, c1In, cMIn);
     __syncthreads();
+    // One CTA barrier per item, between its entry units and its write-back. With two counter
+    // buffers a warp goes from the write-back of one item straight to the units of the next;
+    // with one, a second barrier keeps them apart. Tiles, groups, prefixes, unit counters
+    // and next-item slots alternate by item, so each is rewritten only after the barrier
+    // that follows its last reader.
     while (item < nitems) {
       const uint32_t bcur = kbuf;
+      if (!c.dacc) __syncthreads();
+      uint32_t nx = nitems;
       if (tid == 0) {
-        const uint32_t nx = claim;
-        sMisc[2] = nx;
-        sMisc[3] = 0u;
+        nx = claim;
+        sMisc[8 + bcur] = nx;
         if (nx < nitems) {
           issue(nx, bcur ^ 1u);
           claim = atomicAdd(d.work + t, 1u);
         }
       }
+      // warp 0 loads the next item's groups and prefixes, then joins the entry units
+      // (claimed dynamically)
+      if (warp == 0) {
+        nx = __shfl_sync(kFull, nx, 0);
+        if (nx < nitems) prep(nx, bcur ^ 1u, c1In, cMIn);
+      }
       const uint32_t c0 = item * kRecallCpi;
       const uint32_t parCur = (bcur ? uses1 : uses0) & 1u;
+      // on a timeout the units below run on whatever the buffer holds (in bounds) and the
+      // barrier after them ends the launch
       const bool ok = mbar_wait(&sBar[bcur], parCur, c.waitNs);
       if (bcur) ++uses1; else ++uses0;
-      if (__syncthreads_or(!ok)) {
-        if (tid == 0) {
-          atomicCAS(d.err, 0u, kErrTimeout);
-          // the copies this CTA issued must land before its shared memory is released:
-          // wait for both buffers' outstanding copies, with a bound of its own
-          const uint64_t drain = c.waitNs > kDrainNs ? c.waitNs : kDrainNs;
-          mbar_wait(&sBar[bcur], parCur, drain);
-          if (sMisc[2] < nitems) mbar_wait(&sBar[bcur ^ 1u], (bcur ? uses0 : uses1) & 1u, drain);
-        }
-        __syncthreads();
-        return;
-      }
-      // the next item's groups and prefixes load while this item computes (warps 0 and 1
-      // join the entry units late; the units are claimed dynamically)
-      const uint32_t next = sMisc[2];
-      if (warp < 2 && next < nitems) prep(next, bcur ^ 1u, c1In, cMIn);
+      uint32_t* accB = sAcc + (c.dacc ? bcur * accWords : 0u);
       const uint32_t* cConn = sConn + bcur * 64u;
       const uint32_t* cP1 = sP1 + bcur * 68u;
       const uint32_t* cPM = sPM + bcur * 68u;
@@ -182,7 +185,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       const uint32_t* tileBase = sTile + bcur * kItemWords;
       for (;;) {
         uint32_t u = 0;
-        if (lane == 0) u = atomicAdd(sMisc + 3, 1u);
+        if (lane == 0) u = atomicAdd(sMisc + 6 + bcur, 1u);
         u = __shfl_sync(kFull, u, 0);
         if (u >= units) break;
         uint32_t flat = u * 32u + lane;
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         if (single) {  // one nonzero word: 32 AND-counts
           const uint2 en = __ldcg(e1In + (size_t)g * B + e);
           const uint32_t b = en.x & 0xFFFFu, w = en.x >> 16, S = en.y;
-          uint32_t* accb = sAcc + ((sp >> 5) * B + b) * accStride;
+          uint32_t* accb = accB + ((sp >> 5) * B + b) * accStride;
 #pragma unroll
           for (uint32_t r = 0; r < 32u; r += 4) {
             const uint4 a = *reinterpret_cast<const uint4*>(tile + w3r_pos(r, w));
@@ -211,7 +214,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         } else {  // several nonzero words: counts in registers (words past the third from the spikes)
           const uint4 en = __ldcg(eMIn + (size_t)g * B + e);
           const uint32_t b = en.x & 0xFFFFu, nz = (en.x >> 16) & 0xFFu;
-          uint32_t* accb = sAcc + ((sp >> 5) * B + b) * accStride;
+          uint32_t* accb = accB + ((sp >> 5) * B + b) * accStride;
           uint32_t cnt[32];
 #pragma unroll
           for (int r = 0; r < 32; ++r) cnt[r] = 0u;
@@ -234,7 +237,19 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
                            branch_term<LIN>(cnt[r + 2], dthr, bst), branch_term<LIN>(cnt[r + 3], dthr, bst));
         }
       }
-      __syncthreads();
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicCAS(d.err, 0u, kErrTimeout);
+          // the copies this CTA issued must land before its shared memory is released:
+          // wait for both buffers' outstanding copies, with a bound of its own
+          const uint64_t drain = c.waitNs > kDrainNs ? c.waitNs : kDrainNs;
+          mbar_wait(&sBar[bcur], parCur, drain);
+          if (nx < nitems) mbar_wait(&sBar[bcur ^ 1u], (bcur ? uses0 : uses1) & 1u, drain);
+        }
+        __syncthreads();
+        return;
+      }
+      if (tid == 0) sMisc[6 + bcur] = 0u;  // every warp has claimed its units of this item
       // per-neuron and column drives of the item's columns for every trajectory
       if (PACK && !c.useBias && !c.facil && d.refBall == nullptr) {
         // the packed counters already are the u16 drive slab: four lanes per (column,
@@ -244,7 +259,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         for (uint32_t pp = warp * 8u + grp; pp < kRecallCpi * B; pp += nw * 8u) {
           const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
           if (col >= ncol) continue;  // uniform over the four lanes
-          uint32_t* src = sAcc + (colL * B + b) * accStride + q * 4u;
+          uint32_t* src = accB + (colL * B + b) * accStride + q * 4u;
           const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
           src[0] = src[1] = src[2] = src[3] = 0u;
           reinterpret_cast<uint4*>(d.acc)[(((size_t)b * ncol + col) * 16u >> 2) + q] = w;
@@ -258,7 +273,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         for (uint32_t pp = warp; pp < kRecallCpi * B; pp += nw) {
           const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
           if (col >= ncol) continue;
-          uint32_t* ab = sAcc + (colL * B + b) * accStride;
+          uint32_t* ab = accB + (colL * B + b) * accStride;
           uint32_t a = PACK ? ((ab[lane >> 1] >> (16u * (lane & 1u))) & 0xFFFFu) : ab[lane];
           __syncwarp();
           if (lane < (PACK ? 16u : 32u)) ab[lane] = 0u;
@@ -285,9 +300,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
           }
         }
       }
-      // no barrier here: the next item's first shared-memory writes (counter atomics, the
-      // prefixes of the item after it) come after the next __syncthreads_or
-      item = next;
+      item = sMisc[8 + bcur];
       kbuf ^= 1u;
     }
     if (!grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;
@@ -404,10 +417,10 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   }
 }
 
-size_t recall_smem_bytes(uint32_t ncol, uint32_t B, uint32_t acc32) {
+size_t recall_smem_bytes(uint32_t ncol, uint32_t B, uint32_t acc32, uint32_t dacc) {
   (void)ncol;
   const size_t stride = acc32 ? 33 : 17;
-  return (2ull * kItemWords + kRecallCpi * (size_t)B * stride + 2 * (64 + 68 + 68) + 16 + 4) * 4;
+  return (2ull * kItemWords + (dacc ? 2 : 1) * kRecallCpi * (size_t)B * stride + 2 * (64 + 68 + 68) + 16 + 4) * 4;
 }
 
 namespace {

@@ -38,6 +38,7 @@ struct RecallCfg {
   uint32_t ncol, incols, B, T, clampSteps, useBias, k, dthr, boost, mode, targetCols, facil, biasShift, topkPar;
   uint32_t acc32;  // 1: per-neuron drive kept as u32 (packing two 16-bit sums would overflow)
   uint32_t bst;    // dendritic bonus per branch at or above dthr: boost (mode 1), 0 (mode 0)
+  uint32_t dacc;   // 1: two counter buffers (alternating items), when they fit in shared memory
   uint64_t waitNs;
 };
 
@@ -46,7 +47,7 @@ struct RecallShape {
   size_t smem;
 };
 
-size_t recall_smem_bytes(uint32_t ncol, uint32_t B, uint32_t acc32);
+size_t recall_smem_bytes(uint32_t ncol, uint32_t B, uint32_t acc32, uint32_t dacc);
 cudaError_t recall_max_blocks_per_sm(int acc32, int threads, size_t smem, int* out);
 cudaError_t launch_recall(const RecallDev& d, const RecallCfg& c, const RecallShape& s, cudaStream_t st);
 // W3 [col][s][j][lane][comp] -> W3R [col][s][row = lane][word = 4j + comp]

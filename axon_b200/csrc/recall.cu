@@ -157,7 +157,8 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     rd.err = d.err;
     RecallShape rs{};
     rs.threads = 896;
-    rs.smem = recall_smem_bytes(ncol, Bc, rc.acc32);
+    rc.dacc = recall_smem_bytes(ncol, Bc, rc.acc32, 1u) <= kSmemLimitBytes ? 1u : 0u;
+    rs.smem = recall_smem_bytes(ncol, Bc, rc.acc32, rc.dacc);
     int per_sm = 0;
     CK(recall_max_blocks_per_sm(rc.acc32, rs.threads, rs.smem, &per_sm));
     if (per_sm < 1) return set_error(AXON_EINVAL, "batched recall kernel does not fit one SM");

@@ -98,12 +98,14 @@ def test_recall_batched_equals_plain_full_geometry():
     assert np.array_equal(rb["hist"][idx], h)
 
 
-@pytest.mark.parametrize("B", [149, 320])
+@pytest.mark.parametrize("B", [149, 320, 400])
 def test_recall_several_trajectories_per_cta(B):
     """More trajectories than CTAs (one per SM, 148 on a B200): a CTA selects the
     thresholds of two or three trajectories in turn, the next one's drives loading while
-    the current one is processed. Every trajectory equals the plain method; a sample,
-    including trajectories of a CTA's second and third turn, equals the oracle."""
+    the current one is processed. At 400 trajectories two counter buffers no longer fit in
+    shared memory, and phase 1 keeps one with a second barrier per item. Every trajectory
+    equals the plain method; a sample, including trajectories of a CTA's second and third
+    turn, equals the oracle."""
     cfg, gpu, cpu, pats = trained_pair({}, 6, 3, 16)
     cues = make_cues(pats, cfg.ncol, B, np.random.default_rng(B))
     rb = gpu.recall(cues, 20, 5, hist=True, stats=True)
