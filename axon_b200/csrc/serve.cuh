@@ -68,6 +68,8 @@ struct ServeDev {
   uint32_t slotWords, nactw;
   uint32_t par;              // tick parity: entry lists are read at par and written at par ^ 1
   uint32_t emitParts;        // CTAs sharing one trajectory's emit, each on its own column range
+  uint32_t dacc;             // batched drive with two counter buffers: every batched network of the
+                             // tick has at most serve_batched_dacc_maxb() trajectories
   uint64_t waitNs;           // bound on the batched kernel's copy waits
   uint32_t* err;             // device error word
 };
@@ -88,6 +90,8 @@ __host__ __device__ inline uint32_t serve_slot_words(uint32_t ncol, uint32_t acc
 
 size_t serve_emit_smem_bytes(uint32_t ncol, uint32_t incols);
 size_t serve_batched_smem_bytes(uint32_t packed);
+// most trajectories per network for which the batched drive keeps two counter buffers
+uint32_t serve_batched_dacc_maxb(uint32_t packed);
 cudaError_t serve_prepare(size_t emitSmem);
 cudaError_t serve_batched_prepare(uint32_t packed);
 // drive kernels of one tick (gather for the groups, batched for the batched networks)

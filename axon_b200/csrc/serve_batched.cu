@@ -25,6 +25,16 @@ template <bool PACK>
 __host__ __device__ constexpr uint32_t sb_stride() { return PACK ? 17u : 33u; }
 template <bool PACK>
 __host__ __device__ constexpr uint32_t sb_maxb() { return PACK ? kServeMaxB : kServeMaxB32; }
+// two counter buffers of this many trajectories take about the shared memory one buffer of
+// sb_maxb takes plus what is left of the 227 KiB
+template <bool PACK>
+__host__ __device__ constexpr uint32_t sb_daccb() { return PACK ? 366u : 188u; }
+template <bool PACK>
+__host__ __device__ constexpr uint32_t sb_acc_words() {
+  return 2u * kRecallCpi * sb_daccb<PACK>() * sb_stride<PACK>() > kRecallCpi * sb_maxb<PACK>() * sb_stride<PACK>()
+             ? 2u * kRecallCpi * sb_daccb<PACK>() * sb_stride<PACK>()
+             : kRecallCpi * sb_maxb<PACK>() * sb_stride<PACK>();
+}
 }  // namespace
 
 template <bool PACK, bool LIN>
@@ -32,13 +42,13 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
   extern __shared__ __align__(128) uint32_t sm[];
   const uint32_t ncol = c.ncol, ngrp = ncol / 8u, dthr = c.dthr, bst = c.bst;
   constexpr uint32_t accStride = sb_stride<PACK>();
-  constexpr uint32_t maxB = sb_maxb<PACK>();
   uint32_t* sTile = sm;                                     // [2][kItemWords]
-  uint32_t* sAcc = sTile + 2 * kItemWords;                  // [kRecallCpi][B][accStride]
-  uint32_t* sConn = sAcc + kRecallCpi * maxB * accStride;   // [2][64] groups of the item's branches
+  // counters: one buffer [kRecallCpi][B][accStride], or two of sb_daccb trajectories
+  uint32_t* sAcc = sTile + 2 * kItemWords;
+  uint32_t* sConn = sAcc + sb_acc_words<PACK>();            // [2][64] groups of the item's branches
   uint32_t* sP1 = sConn + 2 * 64;                           // [2][68] single-word entries: prefix over 64 branches
   uint32_t* sPM = sP1 + 2 * 68;                             // [2][68] multi-word entries
-  uint32_t* sMisc = sPM + 2 * 68;                           // [16]
+  uint32_t* sMisc = sPM + 2 * 68;  // [16]: -, first item, -, -, -, -, unit counters [2], next items [2]
   uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
   const uint32_t nip = (ncol + kRecallCpi - 1) / kRecallCpi;  // work items per network
@@ -50,7 +60,7 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
     fence_proxy_async_smem();
   }
   // the counters start at zero; each item's write-back clears what it read
-  for (uint32_t i = tid; i < kRecallCpi * maxB * accStride; i += blockDim.x) sAcc[i] = 0u;
+  for (uint32_t i = tid; i < sb_acc_words<PACK>(); i += blockDim.x) sAcc[i] = 0u;
   __syncthreads();
   uint32_t uses0 = 0, uses1 = 0, kbuf = 0;
 
@@ -63,31 +73,34 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
     for (uint32_t k = 0; k < ncols; ++k)
       bulk_g2s(sTile + buf * kItemWords + k * kColWords, W3R + (size_t)(c0 + k) * kColWords, kColWords * 4u, &sBar[buf]);
   };
-  // warps 0 and 1: the item's branch groups and the prefixes of its 64 entry-list lengths,
-  // single-word (warp 0) and multi-word (warp 1), into buffer buf
+  // warp 0: the item's branch groups and the prefixes of its 64 entry-list lengths, single-
+  // word and multi-word, into buffer buf
   auto prep = [&](uint32_t it, uint32_t buf) {
     const ServeBNet pn = d.bnets[it / nip];
     const uint32_t* conn = d.nets[pn.net].conn;
     const uint32_t* c1 = d.nets[pn.net].ecnt + (size_t)d.par * 2 * ngrp;
+    const uint32_t* cM = c1 + ngrp;
     const uint32_t c0 = (it % nip) * kRecallCpi;
     const bool v1 = c0 + 1 < ncol;
     const uint32_t g0 = __ldg(conn + c0 * kNslot + lane), g1 = v1 ? __ldg(conn + (c0 + 1) * kNslot + lane) : 0u;
-    if (warp == 0) {
-      sConn[buf * 64u + lane] = g0;
-      sConn[buf * 64u + 32u + lane] = g1;
-    }
-    const uint32_t* cin = warp ? c1 + ngrp : c1;
-    uint32_t* P = (warp ? sPM : sP1) + buf * 68u;
-    uint32_t i0 = __ldcg(cin + g0), i1 = v1 ? __ldcg(cin + g1) : 0u;
+    sConn[buf * 64u + lane] = g0;
+    sConn[buf * 64u + 32u + lane] = g1;
+    uint32_t a0 = __ldcg(c1 + g0), a1 = v1 ? __ldcg(c1 + g1) : 0u;
+    uint32_t m0 = __ldcg(cM + g0), m1 = v1 ? __ldcg(cM + g1) : 0u;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-      const uint32_t a = __shfl_up_sync(kFull, i0, off), b = __shfl_up_sync(kFull, i1, off);
-      if (lane >= (uint32_t)off) { i0 += a; i1 += b; }
+      const uint32_t x0 = __shfl_up_sync(kFull, a0, off), x1 = __shfl_up_sync(kFull, a1, off);
+      const uint32_t y0 = __shfl_up_sync(kFull, m0, off), y1 = __shfl_up_sync(kFull, m1, off);
+      if (lane >= (uint32_t)off) { a0 += x0; a1 += x1; m0 += y0; m1 += y1; }
     }
-    const uint32_t tot0 = __shfl_sync(kFull, i0, 31);
-    P[1 + lane] = i0;
-    P[33 + lane] = tot0 + i1;
-    if (lane == 0) P[0] = 0u;
+    const uint32_t totA = __shfl_sync(kFull, a0, 31), totM = __shfl_sync(kFull, m0, 31);
+    uint32_t* P1 = sP1 + buf * 68u;
+    uint32_t* PM = sPM + buf * 68u;
+    P1[1 + lane] = a0;
+    P1[33 + lane] = totA + a1;
+    PM[1 + lane] = m0;
+    PM[33 + lane] = totM + m1;
+    if (lane == 0) P1[0] = PM[0] = 0u;
   };
   auto spk_prev = [&](uint32_t tabOff, uint32_t b) -> const uint32_t* {  // spk(t-1) of batch index b
     const uint2 st = __ldg(d.btab + tabOff + b);
@@ -99,6 +112,7 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
   if (tid == 0) {
     const uint32_t it0 = atomicAdd(d.work, 1u);
     sMisc[1] = it0;
+    sMisc[6] = sMisc[7] = 0u;
     if (it0 < nitems) {
       issue(it0, kbuf);
       claim = atomicAdd(d.work, 1u);
@@ -106,18 +120,30 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
   }
   __syncthreads();
   uint32_t item = sMisc[1];
-  if (warp < 2 && item < nitems) prep(item, kbuf);
+  if (warp == 0 && item < nitems) prep(item, kbuf);
   __syncthreads();
+  // One CTA barrier per item, between its entry units and its write-back. With two counter
+  // buffers a warp goes from the write-back of one item straight to the units of the next;
+  // with one, a second barrier keeps them apart. Tiles, groups, prefixes, unit counters and
+  // next-item slots alternate by item, so each is rewritten only after the barrier that
+  // follows its last reader.
   while (item < nitems) {
     const uint32_t bcur = kbuf;
+    if (!d.dacc) __syncthreads();
+    uint32_t nx = nitems;
     if (tid == 0) {
-      const uint32_t nx = claim;
-      sMisc[2] = nx;
-      sMisc[3] = 0u;
+      nx = claim;
+      sMisc[8 + bcur] = nx;
       if (nx < nitems) {
         issue(nx, bcur ^ 1u);
         claim = atomicAdd(d.work, 1u);
       }
+    }
+    // warp 0 loads the next item's groups and prefixes, then joins the entry units (claimed
+    // dynamically)
+    if (warp == 0) {
+      nx = __shfl_sync(kFull, nx, 0);
+      if (nx < nitems) prep(nx, bcur ^ 1u);
     }
     const ServeBNet bn = d.bnets[item / nip];
     const uint2* e1In = d.nets[bn.net].ent1 + (size_t)d.par * ngrp * kServeMaxB;
@@ -125,23 +151,11 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
     const uint32_t B = bn.B;
     const uint32_t c0 = (item % nip) * kRecallCpi;
     const uint32_t parCur = (bcur ? uses1 : uses0) & 1u;
+    // on a timeout the units below run on whatever the buffer holds (in bounds) and the
+    // barrier after them ends the launch
     const bool ok = mbar_wait(&sBar[bcur], parCur, d.waitNs);
     if (bcur) ++uses1; else ++uses0;
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        atomicCAS(d.err, 0u, kErrTimeout);
-        // the copies this CTA issued must land before its shared memory is released
-        const uint64_t drain = d.waitNs > kDrainNs ? d.waitNs : kDrainNs;
-        mbar_wait(&sBar[bcur], parCur, drain);
-        if (sMisc[2] < nitems) mbar_wait(&sBar[bcur ^ 1u], (bcur ? uses0 : uses1) & 1u, drain);
-      }
-      __syncthreads();
-      return;
-    }
-    // the next item's groups and prefixes load while this item computes (warps 0 and 1
-    // join the entry units late; the units are claimed dynamically)
-    const uint32_t next = sMisc[2];
-    if (warp < 2 && next < nitems) prep(next, bcur ^ 1u);
+    uint32_t* accB = sAcc + (d.dacc ? bcur * (kRecallCpi * sb_daccb<PACK>() * accStride) : 0u);
     const uint32_t* cConn = sConn + bcur * 64u;
     const uint32_t* cP1 = sP1 + bcur * 68u;
     const uint32_t* cPM = sPM + bcur * 68u;
@@ -151,7 +165,7 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
     const uint32_t* tileBase = sTile + bcur * kItemWords;
     for (;;) {
       uint32_t u = 0;
-      if (lane == 0) u = atomicAdd(sMisc + 3, 1u);
+      if (lane == 0) u = atomicAdd(sMisc + 6 + bcur, 1u);
       u = __shfl_sync(kFull, u, 0);
       if (u >= units) break;
       uint32_t flat = u * 32u + lane;
@@ -169,7 +183,7 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
       if (single) {  // one nonzero word: 32 AND-counts
         const uint2 en = __ldcg(e1In + (size_t)g * kServeMaxB + e);
         const uint32_t b = en.x & 0xFFFFu, w = en.x >> 16, S = en.y;
-        uint32_t* accb = sAcc + ((sp >> 5) * B + b) * accStride;
+        uint32_t* accb = accB + ((sp >> 5) * B + b) * accStride;
 #pragma unroll
         for (uint32_t r = 0; r < 32u; r += 4) {
           const uint4 a = *reinterpret_cast<const uint4*>(tile + w3r_pos(r, w));
@@ -180,7 +194,7 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
       } else {  // several nonzero words: counts in registers (words past the third from the spikes)
         const uint4 en = __ldcg(eMIn + (size_t)g * kServeMaxB + e);
         const uint32_t b = en.x & 0xFFFFu, nz = (en.x >> 16) & 0xFFu;
-        uint32_t* accb = sAcc + ((sp >> 5) * B + b) * accStride;
+        uint32_t* accb = accB + ((sp >> 5) * B + b) * accStride;
         uint32_t cnt[32];
 #pragma unroll
         for (int r = 0; r < 32; ++r) cnt[r] = 0u;
@@ -203,7 +217,18 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
                          branch_term<LIN>(cnt[r + 2], dthr, bst), branch_term<LIN>(cnt[r + 3], dthr, bst));
       }
     }
-    __syncthreads();
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicCAS(d.err, 0u, kErrTimeout);
+        // the copies this CTA issued must land before its shared memory is released
+        const uint64_t drain = d.waitNs > kDrainNs ? d.waitNs : kDrainNs;
+        mbar_wait(&sBar[bcur], parCur, drain);
+        if (nx < nitems) mbar_wait(&sBar[bcur ^ 1u], (bcur ? uses0 : uses1) & 1u, drain);
+      }
+      __syncthreads();
+      return;
+    }
+    if (tid == 0) sMisc[6 + bcur] = 0u;  // every warp has claimed its units of this item
     // per-neuron and column drives of the item's columns into every trajectory's slot
     const uint32_t accOff = serve_acc_off(ncol), xOff = 2u * ncol + 2u * d.nactw;
     if (PACK) {  // the packed counters are the u16 drives: four lanes per (column, trajectory),
@@ -214,7 +239,7 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
         const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
         if (col >= ncol) continue;  // uniform over the four lanes
         uint32_t* base = d.slots + (size_t)__ldg(d.btab + bn.tabOff + b).x * d.slotWords;
-        uint32_t* src = sAcc + (colL * B + b) * accStride + q * 4u;
+        uint32_t* src = accB + (colL * B + b) * accStride + q * 4u;
         const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
         src[0] = src[1] = src[2] = src[3] = 0u;
         __stcg(reinterpret_cast<uint4*>(base + accOff + col * 16u) + q, w);
@@ -230,8 +255,8 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
         if (col >= ncol) continue;
         const uint2 st = __ldg(d.btab + bn.tabOff + b);
         uint32_t* base = d.slots + (size_t)st.x * d.slotWords;
-        uint32_t a = sAcc[(colL * B + b) * accStride + lane];
-        sAcc[(colL * B + b) * accStride + lane] = 0u;  // one lane per word
+        uint32_t a = accB[(colL * B + b) * accStride + lane];
+        accB[(colL * B + b) * accStride + lane] = 0u;  // one lane per word
         if (c.facil != 0u && st.y > 0u && ((__ldcg(base + ((st.y - 1u) & 1u) * ncol + col) >> lane) & 1u)) a += c.facil;
         if (c.acc32) __stcg(base + accOff + col * 32u + lane, a);
         else __stcg(reinterpret_cast<unsigned short*>(base + accOff) + col * 32u + lane, (unsigned short)a);
@@ -239,17 +264,17 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
         if (lane == 0) __stcg(base + xOff + col, dsum);
       }
     }
-    // no barrier here: the next item's first shared-memory writes (counter atomics, the
-    // prefixes of the item after it) come after the next __syncthreads_or
-    item = next;
+    item = sMisc[8 + bcur];
     kbuf ^= 1u;
   }
 }
 
 size_t serve_batched_smem_bytes(uint32_t packed) {
-  const size_t maxB = packed ? kServeMaxB : kServeMaxB32, stride = packed ? 17 : 33;
-  return (2ull * kItemWords + kRecallCpi * maxB * stride + 2 * (64 + 68 + 68) + 16 + 4) * 4;
+  const size_t acc = packed ? sb_acc_words<true>() : sb_acc_words<false>();
+  return (2ull * kItemWords + acc + 2 * (64 + 68 + 68) + 16 + 4) * 4;
 }
+
+uint32_t serve_batched_dacc_maxb(uint32_t packed) { return packed ? sb_daccb<true>() : sb_daccb<false>(); }
 
 namespace {
 const void* sb_fn(uint32_t packed, uint32_t lin) {

@@ -340,6 +340,9 @@ axon_status axon_server::tick() {
   td.par = par;
   // few trajectories: several CTAs share each one's emit (the grid has sms * 2 CTAs)
   td.emitParts = ne * 4u <= (uint32_t)sms * 2u ? 4u : (ne * 2u <= (uint32_t)sms * 2u ? 2u : 1u);
+  uint32_t maxBb = 0;
+  for (const ServeBNet& bn : bnH) maxBb = std::max(maxBb, bn.B);
+  td.dacc = maxBb <= serve_batched_dacc_maxb((!cfg.acc32 && cfg.facil == 0u) ? 1u : 0u) ? 1u : 0u;
   CKS(cudaMemcpyAsync(ds, h, bytes, cudaMemcpyHostToDevice, stream));
   const uint32_t eb = pendingEv ^ 1u;  // this tick's events (the previous tick's are still to be read)
   CKS(cudaEventRecord(ev[eb][0], stream));
