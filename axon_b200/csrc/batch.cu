@@ -14,7 +14,9 @@
 //            a lane pops AND-counts of its entry's words against all 32 rows of the tile
 //            and adds the dendritic terms into per-(trajectory, neuron) counters in shared
 //            memory (two 16-bit sums per 32-bit atomic). Silent (branch, trajectory) pairs
-//            cost nothing. The counters then become the per-neuron and column drives.
+//            cost nothing. The counters then become the per-neuron and column drives, and
+//            the write-back that reads them clears them. One CTA barrier per item separates
+//            its units from its write-back; with two counter buffers nothing else does.
 //   phase 2  per trajectory: the column threshold (block_theta), the exact k-of-32 ballot
 //            only for columns that pass the gate, the new spike vector, and its group lists.
 #include <cstdint>
