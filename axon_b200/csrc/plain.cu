@@ -223,12 +223,14 @@ __global__ void __launch_bounds__(kPresentMaxWarps * 32, 1) k_present(NetDev d, 
     if (stamp && tid == 0) stamp[2] = globaltimer_ns();
 
     // ---------------- phase B: column threshold (k_topk) and the full spike vector
-    // drives, this step's drive histogram and the ballots come from L2 by asynchronous
-    // copies; the ballots keep arriving while the threshold is selected
-    for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x)
-      cp_async16(reinterpret_cast<uint4*>(sD) + i, reinterpret_cast<const uint4*>(d.xdrive + par * ncol) + i);
+    // this step's drive histogram, the drives and the ballots come from L2 by asynchronous
+    // copies, in that order (three groups): warp 0 scans the histogram while the drives and
+    // ballots keep arriving
     for (uint32_t i = tid; i < kHistWords / 4u; i += blockDim.x)
       cp_async16(reinterpret_cast<uint4*>(sHist) + i, reinterpret_cast<const uint4*>(xhist + (t % 3u) * kHistWords) + i);
+    cp_async_commit();
+    for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x)
+      cp_async16(reinterpret_cast<uint4*>(sD) + i, reinterpret_cast<const uint4*>(d.xdrive + par * ncol) + i);
     cp_async_commit();
     for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x)
       cp_async16(reinterpret_cast<uint4*>(sB) + i, reinterpret_cast<const uint4*>(d.xball + par * ncol) + i);
@@ -237,9 +239,9 @@ __global__ void __launch_bounds__(kPresentMaxWarps * 32, 1) k_present(NetDev d, 
     // histogram t+2 (last read in step t-1, before this barrier) is cleared for its next use
     if (blockIdx.x == 0 && t >= 1u)
       for (uint32_t i = tid; i < kHistWords; i += blockDim.x) __stcg(xhist + ((t + 2u) % 3u) * kHistWords + i, 0u);
-    cp_async_wait<1>();
+    cp_async_wait<2>();  // the histogram
     __syncthreads();
-    const uint32_t theta = hist_theta(sD, sHist, sCand, sFlag + 2, incols, ncol, c.targetCols, c.topkPar);
+    const uint32_t theta = hist_theta<1>(sD, sHist, sCand, sFlag + 2, incols, ncol, c.targetCols, c.topkPar);
     const uint32_t gate = max(theta, 1u);
     cp_async_wait<0>();
     __syncthreads();

@@ -126,7 +126,11 @@ __device__ __forceinline__ uint32_t theta_key(uint32_t d) {
 // or smallest drive when it ranks first or last in its bin; otherwise the block collects
 // the bin's drives (usually a few) into sCand and warp 0 resolves the rank bit by bit, most
 // significant first. sCtl[0] is the candidate counter and must be zero on entry;
-// sCtl[2..5] is scratch. Every thread of the block calls it.
+// sCtl[2..5] is scratch. Every thread of the block calls it. The histogram must be in shared
+// memory on entry; the drives are read only after the scan, so with kDrivesGroup >= 0 they may
+// still be arriving by asynchronous copy: each thread then waits until at most kDrivesGroup of
+// its copy groups are pending before the block barrier that precedes the first read.
+template <int kDrivesGroup = -1>
 static __device__ __forceinline__ uint32_t hist_theta(const uint32_t* sD, const uint32_t* sH, uint32_t* sCand,
                                                    uint32_t* sCtl, uint32_t incols, uint32_t ncol, uint32_t need,
                                                    uint32_t topkPar) {
@@ -177,6 +181,7 @@ static __device__ __forceinline__ uint32_t hist_theta(const uint32_t* sD, const 
     }
     if (lane == 0u) { sCtl[2] = res; sCtl[3] = b; sCtl[4] = need - above; sCtl[5] = inBin; }
   }
+  if constexpr (kDrivesGroup >= 0) cp_async_wait<kDrivesGroup>();
   __syncthreads();
   const uint32_t res = sCtl[2];
   if (res != 0u) return res;
