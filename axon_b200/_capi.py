@@ -128,6 +128,9 @@ def lib() -> C.CDLL:
         L.axon_inject_missing_arrival.argtypes = [C.c_void_p, C.c_uint32]
         L.axon_stimuli.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, U32P]
         L.axon_load_stim.argtypes = [U32P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, U32P]
+        L.axon_noisy_cue.argtypes = [U32P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, U32P]
+        L.axon_noisy_cue_seed.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
+        L.axon_noisy_cue_seed.restype = C.c_uint32
         L.axon_present_static.argtypes = [C.POINTER(AxonCfg), C.POINTER(StateDev), C.c_uint32, C.c_uint32, C.c_int,
                                           C.c_uint32]
         L.axon_multi_train.argtypes = [C.POINTER(C.c_void_p), C.c_uint32, U32P, U32P, C.POINTER(MultiArgs),

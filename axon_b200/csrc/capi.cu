@@ -1,5 +1,6 @@
 // C ABI of the B200 AXON engine: network objects, device memory and launches.
 // Declarations and per-function reference citations: include/axon_capi.h.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -181,6 +182,22 @@ axon_status axon_load_stim(const uint32_t* cols, uint32_t ncols, double keep, ui
   make_clamp(std::vector<uint32_t>(cols, cols + ncols), keep, seed, ncol, out_ncol);
   return AXON_OK;
 }
+
+axon_status axon_noisy_cue(const uint32_t* cols, uint32_t ncols, double frac, uint32_t seed, uint32_t ncol,
+                           uint32_t* out_ncol) {
+  if ((!cols && ncols) || !out_ncol) return fail(AXON_EINVAL, "bad argument");
+  if (!(frac >= 0.0 && frac <= 1.0)) return fail(AXON_EINVAL, "frac must be in [0, 1]");
+  std::vector<uint32_t> pat(cols, cols + ncols), sorted(pat);
+  std::sort(sorted.begin(), sorted.end());
+  for (uint32_t i = 0; i < ncols; ++i) {
+    if (sorted[i] >= ncol) return fail(AXON_EINVAL, "pattern column out of range");
+    if (i && sorted[i] == sorted[i - 1]) return fail(AXON_EINVAL, "pattern columns must be distinct");
+  }
+  make_noisy_clamp(pat, frac, seed, ncol, out_ncol);
+  return AXON_OK;
+}
+
+uint32_t axon_noisy_cue_seed(uint32_t q, uint32_t pct, uint32_t draw) { return noisy_cue_seed(q, pct, draw); }
 
 axon_status axon_recall(axon_net* net, const uint32_t* cues, uint32_t B, const axon_recall_args* args,
                         const uint32_t* ref_ball, uint32_t* final_spk, uint32_t* hist, uint32_t* stats,

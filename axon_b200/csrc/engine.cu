@@ -31,6 +31,58 @@ std::string validate_cfg(const axon_cfg& c) {
   return "";
 }
 
+PresentCfg make_present_cfg(const axon_cfg& cfg, uint32_t T, uint32_t clampSteps, bool learn, uint32_t useBias,
+                            uint64_t waitNs) {
+  PresentCfg p{};
+  p.ncol = cfg.ncol;
+  p.incols = cfg.incols;
+  p.T = T;
+  p.clampSteps = clampSteps;
+  p.learn = learn ? 1u : 0u;
+  // src/axon.mm:818-822: readout-only k override and facilitation; bias auto = learning
+  p.k = learn ? cfg.k : (cfg.ktest ? cfg.ktest : cfg.k);
+  p.facil = learn ? 0u : cfg.facil;
+  p.useBias = (useBias == 2u) ? (learn ? 1u : 0u) : (useBias ? 1u : 0u);
+  p.dthr = cfg.dthr;
+  p.boost = cfg.boost;
+  p.mode = cfg.mode;
+  p.targetCols = cfg.target;
+  p.biasUp = cfg.biasup;
+  p.biasDown = cfg.biasdown;
+  p.biasShift = cfg.biasshift;
+  p.biasDownEvery = cfg.biasdownevery;
+  p.bandLo = cfg.bandlo;
+  p.bandHi = cfg.contrast ? cfg.bandhi : 0u;  // src/axon.mm:812
+  p.marginGate = cfg.margingate;
+  p.hetero = cfg.hetero;
+  p.ltdRep = cfg.ltdrep;
+  p.contrast = cfg.contrast;
+  p.ltdEvery = cfg.ltdevery ? cfg.ltdevery : 1u;
+  p.topkPar = cfg.topkpar;
+  p.waitNs = waitNs;
+  return p;
+}
+
+axon_status pick_present_shape(uint32_t ncol, uint32_t incols, int sms, LaunchShape* out) {
+  for (int cpw : {1, 2}) {
+    const uint32_t warps = (ncol + cpw - 1) / cpw;
+    int wpb = (int)std::min<uint32_t>(kPresentMaxWarps, (warps + sms - 1) / sms);
+    wpb = std::max(wpb, 1);
+    const int grid = (int)((warps + wpb - 1) / wpb);
+    const size_t smem = present_smem_bytes(ncol, incols, cpw);
+    int per_sm = 0;
+    CK(present_max_blocks_per_sm(cpw, wpb * 32, smem, &per_sm));
+    if (per_sm >= 1 && grid <= per_sm * sms) {
+      out->cpw = cpw;
+      out->wpb = wpb;
+      out->grid = grid;
+      out->smem = smem;
+      return AXON_OK;
+    }
+  }
+  return set_error(AXON_EINVAL, "no co-resident launch shape for this ncol");
+}
+
 }  // namespace axon
 
 axon_status axon_net::create(const axon_cfg& c, int dev) {
@@ -87,28 +139,11 @@ axon_status axon_net::create(const axon_cfg& c, int dev) {
   CK(cudaMallocHost(&hstim, (size_t)ncol * 4));
   CK(cudaMallocHost(&hscratch, 64 * 4));
 
-  // launch shape: one column per warp when the grid fits in one wave, else 2
   cudaDeviceProp prop;
   CK(cudaGetDeviceProperties(&prop, device));
   sm_count = prop.multiProcessorCount;
-  bool ok = false;
-  for (int cpw : {1, 2}) {
-    const uint32_t warps = (ncol + cpw - 1) / cpw;
-    int wpb = (int)std::min<uint32_t>(kPresentMaxWarps, (warps + prop.multiProcessorCount - 1) / prop.multiProcessorCount);
-    wpb = std::max(wpb, 1);
-    const int grid = (int)((warps + wpb - 1) / wpb);
-    shape.smem = present_smem_bytes(ncol, c.incols, cpw);
-    int per_sm = 0;
-    CK(present_max_blocks_per_sm(cpw, wpb * 32, shape.smem, &per_sm));
-    if (per_sm >= 1 && grid <= per_sm * prop.multiProcessorCount) {
-      shape.cpw = cpw;
-      shape.wpb = wpb;
-      shape.grid = grid;
-      ok = true;
-      break;
-    }
-  }
-  if (!ok) return set_error(AXON_EINVAL, "no co-resident launch shape for this ncol");
+  axon_status sst = pick_present_shape(ncol, c.incols, sm_count, &shape);
+  if (sst != AXON_OK) return sst;
   CK(cudaStreamSynchronize(stream));
   return AXON_OK;
 }
@@ -143,34 +178,7 @@ axon_status axon_net::init(uint32_t seed) {
 }
 
 PresentCfg axon_net::present_cfg(uint32_t T, uint32_t clampSteps, bool learn, uint32_t useBias) const {
-  PresentCfg p{};
-  p.ncol = ncol;
-  p.incols = cfg.incols;
-  p.T = T;
-  p.clampSteps = clampSteps;
-  p.learn = learn ? 1u : 0u;
-  // src/axon.mm:818-822: readout-only k override and facilitation; bias auto = learning
-  p.k = learn ? cfg.k : (cfg.ktest ? cfg.ktest : cfg.k);
-  p.facil = learn ? 0u : cfg.facil;
-  p.useBias = (useBias == 2u) ? (learn ? 1u : 0u) : (useBias ? 1u : 0u);
-  p.dthr = cfg.dthr;
-  p.boost = cfg.boost;
-  p.mode = cfg.mode;
-  p.targetCols = cfg.target;
-  p.biasUp = cfg.biasup;
-  p.biasDown = cfg.biasdown;
-  p.biasShift = cfg.biasshift;
-  p.biasDownEvery = cfg.biasdownevery;
-  p.bandLo = cfg.bandlo;
-  p.bandHi = cfg.contrast ? cfg.bandhi : 0u;  // src/axon.mm:812
-  p.marginGate = cfg.margingate;
-  p.hetero = cfg.hetero;
-  p.ltdRep = cfg.ltdrep;
-  p.contrast = cfg.contrast;
-  p.ltdEvery = cfg.ltdevery ? cfg.ltdevery : 1u;
-  p.topkPar = cfg.topkpar;
-  p.waitNs = wait_ns;
-  return p;
+  return make_present_cfg(cfg, T, clampSteps, learn, useBias, wait_ns);
 }
 
 axon_status axon_net::check_device_error() {

@@ -17,6 +17,12 @@ namespace axon {
 axon_status cuda_fail(cudaError_t e, const char* what);
 axon_status set_error(axon_status s, const std::string& msg);
 std::string validate_cfg(const axon_cfg& c);
+// Params of one presentation, as present() resolves them (src/axon.mm:812, 818-845).
+PresentCfg make_present_cfg(const axon_cfg& c, uint32_t T, uint32_t clampSteps, bool learn, uint32_t useBias,
+                            uint64_t waitNs);
+// Co-resident launch shape of k_present for a network of ncol columns on a GPU with `sms`
+// SMs: one column per warp when the grid fits in one wave, else two.
+axon_status pick_present_shape(uint32_t ncol, uint32_t incols, int sms, LaunchShape* out);
 
 }  // namespace axon
 

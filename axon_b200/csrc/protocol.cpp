@@ -50,6 +50,7 @@ struct Cue {
   uint32_t p;
   double keep;
   uint32_t seed;
+  double flip = 0.0;  // > 0: the whole pattern with this fraction of its active bits flipped off
 };
 
 class Session {
@@ -89,7 +90,11 @@ class Session {
     r.T = T_;
     r.ncol = ncol;
     std::vector<uint32_t> words((size_t)r.B * ncol), refw;
-    for (uint32_t b = 0; b < r.B; ++b) make_clamp(pats[cues[b].p], cues[b].keep, cues[b].seed, ncol, &words[(size_t)b * ncol]);
+    for (uint32_t b = 0; b < r.B; ++b) {
+      uint32_t* w = &words[(size_t)b * ncol];
+      if (cues[b].flip > 0.0) make_noisy_clamp(pats[cues[b].p], cues[b].flip, cues[b].seed, ncol, w);
+      else make_clamp(pats[cues[b].p], cues[b].keep, cues[b].seed, ncol, w);
+    }
     if (refs) {
       refw.resize((size_t)r.B * ncol);
       for (uint32_t b = 0; b < r.B; ++b) std::memcpy(&refw[(size_t)b * ncol], (*refs)[b], ncol * 4);
@@ -537,8 +542,13 @@ int Session::run() {
     std::vector<Cue> comp;
     for (double k : keeps)
       for (uint32_t q = 0; q < NSTIM; ++q) comp.push_back({q, k, 4400 + q});
+    // cueflip=P (no counterpart in the reference): one more row, the whole pattern with P%
+    // of its active bits flipped off (axon_noisy_cue, draw 0)
+    const size_t nrows = A.cueflip ? 11 : 10;
+    if (A.cueflip)
+      for (uint32_t q = 0; q < NSTIM; ++q) comp.push_back({q, 1.0, noisy_cue_seed(q, A.cueflip, 0), A.cueflip / 100.0});
     const Readout rcp = readout(comp, T, CLAMP, 0, false, false);
-    for (size_t ki = 0; ki < 10; ++ki) {
+    for (size_t ki = 0; ki < nrows; ++ki) {
       double s1 = 0, o1 = 0, s2 = 0, o2 = 0;
       for (uint32_t q = 0; q < NSTIM; ++q) {
         const Ids a = active_columns(rcp.final_of((uint32_t)(ki * NSTIM + q)), incols, ncol);
@@ -550,8 +560,12 @@ int Session::run() {
         o1 += b1;
         o2 += b2;
       }
-      printf("  %3.0f%% |%25.3f %6.3f %+7.3f |%18.3f %6.3f %+7.3f\n", keeps[ki] * 100, s1 / NSTIM, o1 / NSTIM,
-             s1 / NSTIM - o1 / NSTIM, s2 / NSTIM, o2 / NSTIM, s2 / NSTIM - o2 / NSTIM);
+      if (ki < 10)
+        printf("  %3.0f%% |%25.3f %6.3f %+7.3f |%18.3f %6.3f %+7.3f\n", keeps[ki] * 100, s1 / NSTIM, o1 / NSTIM,
+               s1 / NSTIM - o1 / NSTIM, s2 / NSTIM, o2 / NSTIM, s2 / NSTIM - o2 / NSTIM);
+      else
+        printf("  flip%3u%% |%21.3f %6.3f %+7.3f |%18.3f %6.3f %+7.3f\n", A.cueflip, s1 / NSTIM, o1 / NSTIM,
+               s1 / NSTIM - o1 / NSTIM, s2 / NSTIM, o2 / NSTIM, s2 / NSTIM - o2 / NSTIM);
     }
     printf("======================================================================\n");
   }
@@ -910,7 +924,7 @@ CliArgs CliArgs::parse(int argc, char** argv) {
   g("vtopk", a.vtopk); g("contrast", a.contrast); g("bandlo", a.bandlo); g("bandhi", a.bandhi);
   g("margingate", a.margingate); g("hetero", a.hetero); g("vbs", a.vbs); g("ltdrep", a.ltdrep);
   g("ltdevery", a.ltdevery); g("ktest", a.ktest); g("facil", a.facil); g("deep", a.deep); g("wave", a.wave);
-  g("wavet", a.wavet);
+  g("wavet", a.wavet); g("cueflip", a.cueflip);
   a.trainclamp = argv_u32(argc, argv, "trainclamp", a.contrast ? a.clampsteps : a.T);
   uint32_t dev = argv_u32(argc, argv, "device", 0);
   a.device = (int)dev;
@@ -926,6 +940,7 @@ std::string CliArgs::check() const {
   if (stim == 0) return "stim must be >= 1";
   if (stimcols > incols) return "stimcols must be <= incols";
   if (trainclamp > 64) return "trainclamp must be <= 64";
+  if (cueflip > 100) return "cueflip must be a percentage in 0..100";
   return "";
 }
 

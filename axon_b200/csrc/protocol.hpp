@@ -22,7 +22,8 @@ struct CliArgs {
            stim = 12, quiet = 0, seed = 0, split = 0, unionchar = 0, biasup = 0, biasdown = 1, biasshift = 4,
            biasdownevery = 1, inbr = 8, stimcols = 128, incols = 512, ncol = 4096, diag = 0, profile = 0,
            topkpar = 1, vtopk = 0, contrast = 0, bandlo = 5, bandhi = 11, margingate = 1, hetero = 0, vbs = 0,
-           ltdrep = 1, ltdevery = 1, ktest = 0, facil = 0, deep = 0, wave = 0, wavet = 35, trainclamp = 0;
+           ltdrep = 1, ltdevery = 1, ktest = 0, facil = 0, deep = 0, wave = 0, wavet = 35, trainclamp = 0,
+           cueflip = 0;
   int device = 0;
   static CliArgs parse(int argc, char** argv);
   std::string check() const;  // empty when the run is supported

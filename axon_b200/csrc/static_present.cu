@@ -13,12 +13,17 @@
 // The array is sized for networks of up to kStaticMaxNcol columns; every GPU that loads
 // this library holds it until process exit. The first call on a device looks up the
 // array's device address with cudaGetSymbolAddress (the host-side symbol is only a
-// stand-in and must never be passed to a kernel); make that first call before any stream
-// capture. All calls on a device share the one array, and the kernel leaves the previous
-// call's values in it: the barrier counter and error word are cleared at the start of
-// every call, the exchange slots are fully rewritten before they are read. Calls that
-// overlap on the GPU (other threads, other streams) race on the array and must not be
-// issued.
+// stand-in and must never be passed to a kernel) and keeps it for the life of the
+// process: the library must not outlive a cudaDeviceReset of that device. Every call
+// runs on the legacy default stream and synchronizes with it before returning, so it must
+// not be made while any stream of the device is being captured. Every pointer must be
+// 16-byte aligned (AXON_EINVAL otherwise).
+//
+// All calls on a device share the one array, and the kernel leaves the previous call's
+// values in it: the barrier counter and error word are cleared at the start of every
+// call, the exchange slots are fully rewritten before they are read. Calls that overlap
+// on the GPU (other threads, other streams) race on the array and must not be issued.
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -73,8 +78,13 @@ extern "C" axon_status axon_present_static(const axon_cfg* cfg, const axon_state
   if (use_bias > 2) return set_error(AXON_EINVAL, "use_bias must be 0, 1 or 2");
   const void* need[] = {s->w0, s->w1, s->w2, s->w3, s->conn, s->bias, s->mult, s->refball, s->stim, s->spk_a,
                         s->spk_b, s->drive, s->bbits, s->acc, s->marg, s->drive_log, s->stats, s->hist, s->theta};
-  for (const void* p : need)
+  for (const void* p : need) {
     if (!p) return set_error(AXON_EINVAL, "every device pointer of axon_state_dev is required");
+    // the kernel reads the planes and spike vectors as 16-byte vectors and copies W3 tiles
+    // with cp.async.bulk, whose source must be 16-byte aligned
+    if (((uintptr_t)p & 15u) != 0u)
+      return set_error(AXON_EINVAL, "every device pointer of axon_state_dev must be 16-byte aligned");
+  }
 
   int dev = 0;
   CK(cudaGetDevice(&dev));
@@ -94,38 +104,13 @@ extern "C" axon_status axon_present_static(const axon_cfg* cfg, const axon_state
   d.err = d.bar + 16;
   d.finalOut = nullptr;
 
-  // Params of present(), src/axon.mm:818-845
-  PresentCfg p{};
-  p.ncol = ncol; p.incols = cfg->incols; p.T = T; p.clampSteps = clamp_steps; p.learn = learn ? 1u : 0u;
-  p.k = learn ? cfg->k : (cfg->ktest ? cfg->ktest : cfg->k);
-  p.facil = learn ? 0u : cfg->facil;
-  p.useBias = (use_bias == 2u) ? (learn ? 1u : 0u) : (use_bias ? 1u : 0u);
-  p.dthr = cfg->dthr; p.boost = cfg->boost; p.mode = cfg->mode; p.targetCols = cfg->target;
-  p.biasUp = cfg->biasup; p.biasDown = cfg->biasdown; p.biasShift = cfg->biasshift;
-  p.biasDownEvery = cfg->biasdownevery; p.bandLo = cfg->bandlo; p.bandHi = cfg->contrast ? cfg->bandhi : 0u;
-  p.marginGate = cfg->margingate; p.hetero = cfg->hetero; p.ltdRep = cfg->ltdrep; p.contrast = cfg->contrast;
-  p.ltdEvery = cfg->ltdevery ? cfg->ltdevery : 1u; p.topkPar = cfg->topkpar; p.waitNs = 2000000000ull;
-
-  // co-resident launch shape (same rule as axon_create)
+  // Params of present() and the co-resident launch shape: the same helpers axon_net uses
+  const PresentCfg p = make_present_cfg(*cfg, T, clamp_steps, learn != 0, use_bias, 2000000000ull);
   int sms = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   LaunchShape ls{};
-  bool ok = false;
-  for (int cpw : {1, 2}) {
-    const uint32_t warps = (ncol + cpw - 1) / cpw;
-    int wpb = (int)((warps + sms - 1) / sms);
-    wpb = wpb < 1 ? 1 : (wpb > (int)kPresentMaxWarps ? (int)kPresentMaxWarps : wpb);
-    const int grid = (int)((warps + wpb - 1) / wpb);
-    ls.smem = present_smem_bytes(ncol, cfg->incols, cpw);
-    int per_sm = 0;
-    CK(present_max_blocks_per_sm(cpw, wpb * 32, ls.smem, &per_sm));
-    if (per_sm >= 1 && grid <= per_sm * sms) {
-      ls.cpw = cpw; ls.wpb = wpb; ls.grid = grid;
-      ok = true;
-      break;
-    }
-  }
-  if (!ok) return set_error(AXON_EINVAL, "no co-resident launch shape for this ncol");
+  st = pick_present_shape(ncol, cfg->incols, sms, &ls);
+  if (st != AXON_OK) return st;
 
   // clear what the kernel expects at zero: stats (launch_present clears the barrier
   // region, error word included)

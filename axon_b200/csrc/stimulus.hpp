@@ -69,4 +69,31 @@ inline void make_clamp(const std::vector<uint32_t>& pattern, double keep, uint32
     if (rng.unit() <= keep) out[c] = 0xFFFFFFFFu;
 }
 
+// Noisy cue: the clamp words of the whole pattern (every pattern column on), then
+// round(frac * A) of its A = 32 * pattern.size() active bits flipped off. The active bits
+// are listed column by column in pattern order, bit 0 first; the flipped ones are the
+// first picks of a forward Fisher-Yates over that list driven by mt19937(seed), each pick
+// i + U[0, A-1-i] drawn as the shuffle above draws (so the picks for a smaller fraction
+// are the first picks for a larger one with the same seed). Pattern columns must be
+// distinct and below ncol.
+inline void make_noisy_clamp(const std::vector<uint32_t>& pattern, double frac, uint32_t seed, uint32_t ncol,
+                             uint32_t* out) {
+  for (uint32_t c = 0; c < ncol; ++c) out[c] = 0u;
+  for (uint32_t c : pattern) out[c] = 0xFFFFFFFFu;
+  const uint64_t A = 32ull * pattern.size();
+  uint64_t nflip = (uint64_t)(frac * (double)A + 0.5);
+  if (nflip > A) nflip = A;
+  std::vector<uint32_t> idx(A);
+  for (uint64_t i = 0; i < A; ++i) idx[i] = (uint32_t)i;
+  StimulusRng rng(seed);
+  for (uint64_t i = 0; i < nflip; ++i) {
+    const uint64_t j = i + rng.below(A - i);
+    std::swap(idx[i], idx[j]);
+    out[pattern[idx[i] >> 5]] &= ~(1u << (idx[i] & 31u));
+  }
+}
+
+// Seed of noisy-cue draw `draw` of pattern q at `pct` percent of active bits flipped.
+inline uint32_t noisy_cue_seed(uint32_t q, uint32_t pct, uint32_t draw) { return 90000u + 1000u * pct + 16u * q + draw; }
+
 }  // namespace axon

@@ -303,6 +303,20 @@ def load_stim(cols: np.ndarray, keep: float, seed: int, ncol: int) -> np.ndarray
     return out
 
 
+def noisy_cue(cols: np.ndarray, frac: float, seed: int, ncol: int) -> np.ndarray:
+    """Clamp words of the whole pattern with round(frac * 32 * len(cols)) of its active bits
+    flipped off, chosen from a seeded stream (axon_noisy_cue)."""
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    out = np.empty(ncol, dtype=np.uint32)
+    A.check(A.lib().axon_noisy_cue(A.u32(cols), cols.size, C.c_double(frac), seed, ncol, A.u32(out)))
+    return out
+
+
+def noisy_cue_seed(q: int, pct: int, draw: int) -> int:
+    """Seed of draw `draw` of pattern q's noisy cue at `pct` percent flipped (axon_noisy_cue_seed)."""
+    return int(A.lib().axon_noisy_cue_seed(q, pct, draw))
+
+
 def bstest(op: int, lo: int, hi: int, planes: list[np.ndarray], mask: np.ndarray, device: int = 0) -> None:
     """Runs the bit-serial inc/dec/clip kernel in place on four planes (k_bstest)."""
     ps = [np.ascontiguousarray(p, dtype=np.uint32) for p in planes]

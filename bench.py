@@ -2,10 +2,12 @@
 
 Workload (the batched-recall configuration): config C network (131,072 neurons, 512 MiB of
 4-bit counters), 60 patterns, seed 0, trained for 40 epochs by the plain GPU path (setup,
-untimed). 300 cues = the 60 stored patterns plus noisy variants in which a fraction 0.1 or
-0.25 of each pattern's 64 columns is moved to other input columns (2 seeded draws each).
-Every trajectory is 10 clamped + 35 free steps with the intrinsic bias off (the reference's
-readout setting). One bench step = one batched recall of all 300 trajectories.
+untimed). 300 cues = the 60 whole stored patterns plus, for each fraction 10 % and 25 % and
+two seeded draws each, the patterns with that fraction of their active cue bits flipped off
+(axon_noisy_cue). Every trajectory is 10 clamped + 35 free steps with the intrinsic bias off
+(the reference's readout setting). One bench step = one batched recall of all 300
+trajectories. The trained planes and all 300 trajectories are checked against the CPU
+oracle's answer for this workload (tests/golden/recall_load60.json).
 
 Synaptic event: one presynaptic spike delivered to one postsynaptic neuron through conn,
 i.e. per step sum over (column, branch) of 32 * popcount(spikes of the branch's group at
@@ -16,6 +18,7 @@ t-1). The count is fixed by the workload (identical for every method and for the
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import subprocess
@@ -31,44 +34,47 @@ sys.path.insert(0, str(ROOT))
 
 NCOL, INCOLS, STIMCOLS, LOAD, EPOCHS, SEED = 4096, 512, 64, 60, 40, 0
 T_RECALL, CLAMP_RECALL = 45, 10
-FLIPS = (0.10, 0.25)
-DRAWS = 2
+T_WAVE, CLAMP_WAVE = 35, 5  # the reference's wave readout: 5 clamped + 30 free steps
+FLIP_PCTS, DRAWS = (10, 25), 2
 L2_BYTES = 126 * 2 ** 20
+GOLDEN = ROOT / "tests" / "golden" / "recall_load60.json"
+PUBLISHED = ROOT / "tests" / "golden" / "published.json"
+# config C as CLI keys (bench/cap10.sh:7)
+CONFIG_C_KEYS = dict(nand=4, target=64, k=24, dthr=1, mode=1, inbr=4, contrast=1, margingate=0, ltdrep=1, ltdevery=2,
+                     biasup=73, biasdown=1)
 
 
-def config_c():
-    import axon_b200 as ax
-
-    return ax.config(ncol=NCOL, incols=INCOLS, **ax.CONFIG_C)
-
-
-def noisy_cue(pattern: np.ndarray, frac: float, seed: int, rng_cls=np.random.default_rng) -> np.ndarray:
-    """Clamp words of a pattern with round(frac * len) of its columns moved to input
-    columns outside the pattern (seeded)."""
-    rng = rng_cls(seed)
-    n = len(pattern)
-    nflip = int(round(frac * n))
-    out_cols = rng.choice(n, nflip, replace=False)
-    others = np.setdiff1d(np.arange(INCOLS), pattern)
-    new = rng.choice(others, nflip, replace=False)
-    cols = pattern.copy()
-    cols[out_cols] = new
-    stim = np.zeros(NCOL, dtype=np.uint32)
-    stim[cols] = 0xFFFFFFFF
-    return stim
-
-
-def make_cues(pats: np.ndarray) -> np.ndarray:
-    cues = []
-    for q in range(LOAD):
-        stim = np.zeros(NCOL, dtype=np.uint32)
-        stim[pats[q]] = 0xFFFFFFFF
-        cues.append(stim)
-    for fi, f in enumerate(FLIPS):
+def make_cues(pats: np.ndarray, noisy_cue, noisy_seed) -> np.ndarray:
+    """The 300 cues in batch order: the 60 whole patterns, then per fraction and draw the 60
+    noisy ones (noisy_cue / noisy_seed from the engine's C ABI, or the oracle's)."""
+    cues = [noisy_cue(pats[q], 0.0, 0, NCOL) for q in range(LOAD)]
+    for pct in FLIP_PCTS:
         for d in range(DRAWS):
-            for q in range(LOAD):
-                cues.append(noisy_cue(pats[q], f, 90000 + q * 16 + fi * 4 + d))
+            cues += [noisy_cue(pats[q], pct / 100.0, noisy_seed(q, pct, d), NCOL) for q in range(LOAD)]
     return np.stack(cues)
+
+
+def digest(*arrays: np.ndarray, n: int | None = None) -> str:
+    """SHA-256 of the arrays' words (little-endian), as the fixture records them."""
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a, dtype="<u4").tobytes())
+    return h.hexdigest()[:n] if n else h.hexdigest()
+
+
+def fixture() -> dict | None:
+    return json.loads(GOLDEN.read_text()) if GOLDEN.exists() else None
+
+
+def check_against_fixture(fx: dict | None, idx, hists) -> dict:
+    """Trajectories idx (their (T, ncol) spike histories) against the oracle's fixture."""
+    if fx is None:
+        return {"checked": 0, "mismatches": None, "source": "fixture missing"}
+    rows = fx["trajectories"]
+    idx = [int(b) for b in idx]
+    bad = [b for b, h in zip(idx, hists) if digest(h, n=16) != rows[b]["hist"] or digest(h[-1], n=16) != rows[b]["final"]]
+    return {"checked": len(idx), "mismatches": len(bad), "first_mismatch": bad[0] if bad else None,
+            "source": "tests/golden/recall_load60.json (CPU oracle)"}
 
 
 def events_per_step(hist: np.ndarray, conn: np.ndarray) -> np.ndarray:
@@ -81,22 +87,58 @@ def events_per_step(hist: np.ndarray, conn: np.ndarray) -> np.ndarray:
     return ev
 
 
+def train(net, pats, load_stim) -> float:
+    """The reference's training schedule (src/axon.mm:1009-1033) on `net` (engine or oracle)."""
+    t0 = time.time()
+    for _ in range(EPOCHS):
+        for p in range(LOAD):
+            net.present(load_stim(pats[p], 1.0, 1000 + p, NCOL), 10, 5, True)
+    net.present(load_stim(pats[0], 1.0, 31337, NCOL), 10, 5, True)  # the reference's extra presentation
+    return time.time() - t0
+
+
+def trained_digest(net) -> str:
+    return digest(*(net.read(n) for n in ("W0", "W1", "W2", "W3", "BIAS")))
+
+
 MULTI_SEEDS, MULTI_LOADS = (0, 1, 2, 3, 4), (12, 24, 36, 48, 60)
+
+
+def config_c():
+    import axon_b200 as ax
+
+    return ax.config(ncol=NCOL, incols=INCOLS, **ax.CONFIG_C)
 
 
 def printed(r: dict) -> dict:
     """One network's measurements as the command line prints them."""
     first, last = float(f"{r['wave_first']:.3f}"), float(f"{r['wave_last']:.3f}")
-    return {"within": f"{r['within_pct']:.2f}", "recall": f"{r['recall']:.3f}", "best_other": f"{r['best_other']:.3f}",
-            "margin": f"{r['recall'] - r['best_other']:+.3f}", "sustained": f"{last / first:.3f}",
-            "drive": f"{r['drive_t6']:.0f}"}
+    return {"within": f"{r['within_pct']:.2f}", "within_pct": f"{r['within_pct']:.4f}", "recall": f"{r['recall']:.3f}",
+            "best_other": f"{r['best_other']:.3f}", "margin": f"{r['recall'] - r['best_other']:+.3f}",
+            "sustained": f"{last / first:.3f}", "drive": f"{r['drive_t6']:.0f}"}
 
 
-def bench_multi(dev: int, nnets: int = 25, epochs: int = EPOCHS) -> dict:
+def published() -> dict:
+    return json.loads(PUBLISHED.read_text())
+
+
+def table1_equal(rows: dict) -> dict:
+    """Per load: do the printed measurements equal the published Table 1 row?"""
+    gold = {r["stim"]: r for r in published()["table1"]}
+    keys = ("within", "recall", "best_other", "margin", "sustained", "drive")
+    return {str(L): all(m[k] == gold[L][k] for k in keys) for L, m in rows.items() if L in gold}
+
+
+def bench_multi(dev: int, nnets: int = 25, epochs: int = EPOCHS, pins: bool = True) -> dict:
     """25 networks of uneven load (seeds 0-4 x loads 12..60, config C, 40 epochs plus the
     readouts of the five measurements): one persistent launch with an autotuned shape,
-    against the plain path running the same presentations one launch each."""
+    against the plain path running the same presentations one launch each. The seed-0
+    rows are compared with the published Table 1 and the five-seed summaries with Table 2
+    (its load 42 from five more networks, outside the timed workload), and seed-0 networks
+    at Table 1's higher loads are trained and compared too (140 and 200, the loads of the
+    serving networks, in one launch; 74, 90 and 300 through the plain path)."""
     import axon_b200 as ax
+    from tests.metrics import seeds_summary
 
     seeds = [s for s in MULTI_SEEDS for _ in MULTI_LOADS][:nnets]
     loads = [L for _ in MULTI_SEEDS for L in MULTI_LOADS][:nnets]
@@ -109,8 +151,6 @@ def bench_multi(dev: int, nnets: int = 25, epochs: int = EPOCHS) -> dict:
         for n in nets:
             n.close()
     assert res_m == res_p, "one-launch measurements differ from the plain path"
-    gold = {r["stim"]: {k: r[k] for k in ("within", "recall", "best_other", "margin", "sustained", "drive")}
-            for r in json.loads((ROOT / "tests" / "golden" / "published.json").read_text())["table1"]}
     rows = {L: printed(res_m[i]) for i, (s, L) in enumerate(zip(seeds, loads)) if s == 0}
     steps = rep_m["steps"]
     # algorithmic HBM bytes of the launch: W3 tiles read by the drive, branch updates of
@@ -120,30 +160,66 @@ def bench_multi(dev: int, nnets: int = 25, epochs: int = EPOCHS) -> dict:
            + rep_m["train_steps"] * 1024.0 * 1024.0)
     hbm_peak, pk = peaks()
     achieved = alg / (rep_m["gpu_ms"] / 1e3) / 1e9
-    return {"workload": f"{len(nets)} networks (seeds 0-4 x loads 12,24,36,48,60), config C, {epochs} epochs + readouts",
-            "networks": len(nets), "network_steps": steps, "learning_steps": rep_m["train_steps"],
-            "one_launch_ms": rep_m["gpu_ms"], "plain_ms": rep_p["gpu_ms"],
-            "one_launch_steps_per_s": steps / (rep_m["gpu_ms"] / 1e3),
-            "plain_steps_per_s": steps / (rep_p["gpu_ms"] / 1e3), "speedup_vs_plain": rep_p["gpu_ms"] / rep_m["gpu_ms"],
-            "shape": {k: rep_m[k] for k in ("slots", "threads", "tiles", "grid", "graph", "tried")},
-            "tune_ms": rep_m["tune_ms"], "bit_exact_vs_plain": True,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                         "peak_kind": pk, "w3_tiles": rep_m["w3_tiles"], "learn_tasks": rep_m["learn_tasks"],
-                         "note": "algorithmic bytes = 1 KiB per W3 tile read + 8 KiB per learning branch update + "
-                                 "conn/spikes per step + bias per learning step"},
-            "seed0_rows": rows,
-            "seed0_rows_equal_published_table1": epochs == EPOCHS and all(rows[L] == gold[L] for L in rows)}
+    out = {"workload": f"{len(nets)} networks (seeds 0-4 x loads 12,24,36,48,60), config C, {epochs} epochs + readouts",
+           "networks": len(nets), "network_steps": steps, "learning_steps": rep_m["train_steps"],
+           "one_launch_ms": rep_m["gpu_ms"], "plain_ms": rep_p["gpu_ms"],
+           "one_launch_steps_per_s": steps / (rep_m["gpu_ms"] / 1e3),
+           "plain_steps_per_s": steps / (rep_p["gpu_ms"] / 1e3), "speedup_vs_plain": rep_p["gpu_ms"] / rep_m["gpu_ms"],
+           "shape": {k: rep_m[k] for k in ("slots", "threads", "tiles", "grid", "graph", "tried")},
+           "tune_ms": rep_m["tune_ms"], "bit_exact_vs_plain": True,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                        "peak_kind": pk, "w3_tiles": rep_m["w3_tiles"], "learn_tasks": rep_m["learn_tasks"],
+                        "note": "algorithmic bytes = 1 KiB per W3 tile read + 8 KiB per learning branch update + "
+                                "conn/spikes per step + bias per learning step"},
+           "seed0_rows": rows}
+    if epochs != EPOCHS or nnets != 25 or not pins:
+        return out
+    eq = table1_equal(rows)
+    out["seed0_rows_equal_published_table1"] = all(eq.values())
+    # Table 2: five-seed summaries; load 42 from five more networks
+    per = {L: [printed(res_m[i]) for i, (s, LL) in enumerate(zip(seeds, loads)) if LL == L] for L in MULTI_LOADS}
+    nets = [ax.Network(config_c(), device=dev) for _ in MULTI_SEEDS]
+    try:
+        r42, _ = ax.multi_train(nets, list(MULTI_SEEDS), [42] * 5, method="plain", **kw)
+    finally:
+        for n in nets:
+            n.close()
+    per[42] = [printed(r) for r in r42]
+    summ = {str(L): seeds_summary(v) for L, v in sorted(per.items())}
+    t2 = {str(r["stim"]): r for r in published()["table2"]["rows"]}
+    fields = ("sustained_mean", "sustained_sd", "margin_mean", "margin_sd", "within_mean", "within_sd")
+    out["table2"] = {"summary": summ, "equal_published": {L: all(summ[L][f] == t2[L][f] for f in fields) for L in t2}}
+    out["table2"]["stim12_sustained_mean_equal_published"] = summ["12"]["sustained_mean"] == published()["table2"][
+        "stim12_sustained_mean"]
+    out["seed_means_equal_table2"] = all(out["table2"]["equal_published"].values())
+    # Table 1 at the higher loads, seed 0
+    hi = {}
+    for method, lds in (("launch", [140, 200]), ("plain", [74, 90, 300])):
+        nets = [ax.Network(config_c(), device=dev) for _ in lds]
+        try:
+            r, rep = ax.multi_train(nets, [0] * len(lds), lds, method=method, autotune=method == "launch", **kw)
+        finally:
+            for n in nets:
+                n.close()
+        hi.update({L: printed(x) for L, x in zip(lds, r)})
+    out["table1_high_loads"] = {"rows": {str(L): hi[L] for L in sorted(hi)}, "equal_published": table1_equal(hi),
+                                "methods": {"one launch": [140, 200], "plain": [74, 90, 300]}}
+    return out
 
 
 SERVE_LOADS = (12, 36, 60, 100, 140, 170, 200, 200)
 SERVE_RATES = (2000, 10000, 50000)
 SERVE_SECONDS = 1.0
+SERVE_CHECK = {2000: None, 10000: 1000, 50000: 1000}  # requests checked against a plain recall (None = all)
 
 
 def bench_serve(dev: int, rates=SERVE_RATES, seconds: float = SERVE_SECONDS, nnets: int = len(SERVE_LOADS)) -> dict:
     """Recall serving: 8 trained networks (config C, loads 12..200, seeds 0-7) answer
     Poisson-arriving recall requests (cue = 16-64 of a stored pattern's columns, 5 clamped
-    + 10-60 free steps) with continuous batching; latency = result on the host - arrival."""
+    + 10-60 free steps) with continuous batching; latency = result on the host - arrival.
+    After each rate's run (outside its timed window) every request at 2,000 req/s, and
+    1,000 spread over the others, are recomputed one at a time through the plain path and
+    compared with the server's result."""
     import axon_b200 as ax
 
     loads = list(SERVE_LOADS[:nnets])
@@ -161,12 +237,12 @@ def bench_serve(dev: int, rates=SERVE_RATES, seconds: float = SERVE_SECONDS, nne
         out = {"workload": f"{len(nets)} networks (config C, loads {','.join(map(str, loads))}, seeds 0-{len(nets) - 1}); "
                            "Poisson arrivals; cue 16-64 columns of a stored pattern; 5 clamped + 10-60 free steps",
                "train_ms": rep["gpu_ms"], "rates": []}
-        srv = ax.Server(nets, 1 << 30)
-        try:
-            out["slots"] = srv.stats()["slots"]
-            rng = np.random.default_rng(12345)
-            tag = 0
-            for rate in rates:
+        rng = np.random.default_rng(12345)
+        tag = 0
+        for rate in rates:
+            srv = ax.Server(nets, 1 << 30)
+            try:
+                out["slots"] = srv.stats()["slots"]
                 n = int(rate * seconds)
                 gaps = rng.exponential(1.0 / rate, n)
                 reqs = []
@@ -180,9 +256,9 @@ def bench_serve(dev: int, rates=SERVE_RATES, seconds: float = SERVE_SECONDS, nne
                 arrive = t0 + np.cumsum(gaps)
                 for (tg, net, q, cols, free), a in zip(reqs, arrive):
                     srv.submit(net, cols, 5, free, tg, float(a))
-                sample = {r[0]: r for r in reqs[:: max(1, n // 16)]}
-                lat, ov, first, last, got, exact = [], [], None, 0.0, 0, True
+                lat, ov, last, got = [], [], 0.0, 0
                 info = {r[0]: r for r in reqs}
+                results = {}
                 while got < n:
                     done = srv.poll(4096)
                     if not done:
@@ -195,22 +271,26 @@ def bench_serve(dev: int, rates=SERVE_RATES, seconds: float = SERVE_SECONDS, nne
                         act = set(np.nonzero(spk[INCOLS:])[0].tolist())
                         ref = refs[net][q]
                         ov.append(len(act & ref) / np.sqrt(len(act) * len(ref)) if act and ref else 0.0)
-                        if res["tag"] in sample:
-                            alone = nets[net].recall(ax.clamp_words(cols, NCOL)[None, :], 5 + free, 5,
-                                                     method="plain")["final"][0]
-                            exact &= bool(np.array_equal(alone, spk))
+                        results[res["tag"]] = spk
                     got += len(done)
                 st = srv.stats()
-                lat_ms = np.array(lat) * 1e3
-                out["rates"].append({"offered_req_s": rate, "requests": n,
-                                     "trajectories_per_s": n / (last - float(arrive[0])),
-                                     "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
-                                     "mean_overlap_with_reference": float(np.mean(ov)),
-                                     "sample_bit_exact_vs_alone": exact, "sample": len(sample),
-                                     "mean_batch_so_far": st["mean_batch"], "max_batch_so_far": st["max_batch"]})
-                tag += n
-        finally:
-            srv.close()
+            finally:
+                srv.close()
+            # after the timed window: each checked request alone through the plain path
+            ncheck = n if SERVE_CHECK.get(rate) is None else min(n, SERVE_CHECK[rate])
+            checked = reqs[:: max(1, n // ncheck)][:ncheck]
+            mism = 0
+            for tg, net, q, cols, free in checked:
+                alone = nets[net].recall(ax.clamp_words(cols, NCOL)[None, :], 5 + free, 5, method="plain")["final"][0]
+                mism += int(not np.array_equal(alone, results[tg]))
+            lat_ms = np.array(lat) * 1e3
+            out["rates"].append({"offered_req_s": rate, "requests": n,
+                                 "trajectories_per_s": n / (last - float(arrive[0])),
+                                 "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+                                 "mean_overlap_with_reference": float(np.mean(ov)),
+                                 "checked": len(checked), "mismatches": mism,
+                                 "mean_batch": st["mean_batch"], "max_batch": st["max_batch"]})
+            tag += n
     finally:
         for x in nets:
             x.close()
@@ -229,15 +309,51 @@ def plain_alg_bytes(hist: np.ndarray, conn: np.ndarray) -> float:
     return float((1024.0 * tiles + 512 * 1024 + 16 * 1024).sum())
 
 
-def train(net, pats) -> float:
-    import axon_b200 as ax
+def cli_args() -> list[str]:
+    return [f"{k}={v}" for k, v in CONFIG_C_KEYS.items()] + ["stimcols=64", "T=10", "clampsteps=5"]
 
-    t0 = time.time()
-    for ep in range(EPOCHS):
-        for p in range(LOAD):
-            net.present(ax.load_stim(pats[p], 1.0, 1000 + p, NCOL), 10, 5, True)
-    net.present(ax.load_stim(pats[0], 1.0, 31337, NCOL), 10, 5, True)  # the reference's extra presentation
-    return time.time() - t0
+
+def plain_train(dev: int, threads: int) -> dict:
+    """The reference's one published throughput, config C timesteps/s while training
+    (paper/axon_preprint.tex:667-669: 2,554-2,956 on an M1 Pro), measured as the reference
+    measures it: the drop-in command line at loads 12-60, 40 epochs, seed 0, printing its
+    'ms/timestep -> N steps/s' line and the five measurements (compared with Table 1).
+    Beside it, the CPU oracle's training steps/s on the host cores over one epoch of
+    load 12 (a bounded sample of the same presentations)."""
+    from axon_b200 import build
+    from tests.metrics import scrape
+
+    exe = build.build_cli()
+    rows = {}
+    for L in MULTI_LOADS:
+        t0 = time.time()
+        p = subprocess.run([str(exe), *cli_args(), f"stim={L}", "epochs=40", "seed=0", "deep=1", "wave=1", "wavet=35",
+                            f"device={dev}"], capture_output=True, text=True, timeout=900)
+        if p.returncode != 0:
+            raise RuntimeError(p.stderr)
+        m = scrape(p.stdout)
+        rows[L] = {"steps_per_s": float(m["steps_per_s"]), "wall_s": round(time.time() - t0, 2),
+                   "within": f"{float(m['within_pct']):.2f}", "recall": m["recall"], "best_other": m["best_other"],
+                   "margin": m["margin"], "sustained": m["sustained"], "drive": m["drive_t6"]}
+    eq = table1_equal({L: r for L, r in rows.items()})
+    # CPU oracle: one epoch of load-12 learning presentations on the host cores
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib as O
+
+    cpu = O.OracleNet(O.config(ncol=NCOL, incols=INCOLS, **CONFIG_C_KEYS), threads=threads)
+    cpu.init(SEED)
+    pats = O.stimuli(SEED, 12, INCOLS, STIMCOLS)
+    t0 = time.perf_counter()
+    for p in range(12):
+        cpu.present(O.load_stim(pats[p], 1.0, 1000 + p, NCOL), 10, 5, True)
+    cpu_s = time.perf_counter() - t0
+    cpu.close()
+    return {"workload": "config C training, 40 epochs, seed 0, through the axon command line (drop-in)",
+            "steps_per_s": {str(L): r["steps_per_s"] for L, r in rows.items()}, "rows": {str(L): r for L, r in rows.items()},
+            "rows_equal_table1": eq,
+            "published_m1_pro_steps_per_s": "2554-2956 (paper/axon_preprint.tex:667-669; context only, not on this box)",
+            "cpu_oracle": {"steps_per_s": 120 / cpu_s, "cores": threads,
+                           "sample": "1 epoch of load 12 (12 learning presentations x 10 steps)"}}
 
 
 class ClockSampler:
@@ -296,26 +412,35 @@ def peaks() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def cpu_sample(cfg, gpu_net, cues, ev, threads: int, ntraj: int) -> dict:
-    """The CPU oracle on a bounded sample of the same trajectories (same trained state)."""
+def cpu_sample(gpu_net, cues, ev, gpu_hist, threads: int, ntraj: int) -> dict:
+    """The CPU oracle on a bounded sample of the same trajectories (same trained state),
+    timed, and each sampled trajectory compared with the GPU's spike history."""
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle_lib as O
 
-    cpu = O.OracleNet(cfg, threads=threads)
+    cpu = O.OracleNet(O.config(ncol=NCOL, incols=INCOLS, **CONFIG_C_KEYS), threads=threads)
     for name in ("W0", "W1", "W2", "W3", "CONN", "BIAS"):
         cpu.write(name, gpu_net.read(name))
     idx = np.linspace(0, cues.shape[0] - 1, ntraj).astype(int)
-    t0 = time.perf_counter()
+    dt, mism = 0.0, 0
     for b in idx:
+        t0 = time.perf_counter()
         cpu.present(cues[b], T_RECALL, CLAMP_RECALL, False, True, 0)
-    dt = time.perf_counter() - t0
+        dt += time.perf_counter() - t0
+        h = cpu.read("HIST")[: T_RECALL * NCOL].reshape(T_RECALL, NCOL)
+        mism += int(not np.array_equal(h, gpu_hist[b]))
     cpu.close()
     return {"value": float(ev[idx].sum() / dt), "unit": "synaptic events/s", "cores": threads, "kind": "port",
-            "sample": f"{ntraj} of the 300 trajectories x {T_RECALL} steps, oracle present(learn=0), {dt:.1f} s"}
+            "sample": f"{ntraj} of the 300 trajectories (evenly spread over clean and noisy cues) x {T_RECALL} steps, "
+                      f"oracle present(learn=0), {dt:.1f} s",
+            "oracle_match": {"checked": int(ntraj), "mismatches": mism, "compared": "full spike history vs the GPU's"}}
 
 
 def run_reference(args) -> None:
-    """Reference arm: the CPU restatement of the reference (oracle) on the host cores."""
+    """Reference arm: the CPU restatement of the reference (oracle) on the host cores. It
+    loads nothing from the engine: configuration, patterns and cues come from the oracle
+    library alone. Its trained planes and its sampled trajectories are checked against the
+    oracle fixture of this workload, the same fixture the GPU arm is checked against."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -323,23 +448,20 @@ def run_reference(args) -> None:
     import oracle_lib as O
 
     threads = os.cpu_count() or 1
-    cfg = config_c()
+    cfg = O.config(ncol=NCOL, incols=INCOLS, **CONFIG_C_KEYS)
     pats = O.stimuli(SEED, LOAD, INCOLS, STIMCOLS)
-    cues = make_cues(pats)
+    cues = make_cues(pats, O.noisy_cue, O.noisy_seed)
     cpu = O.OracleNet(cfg, threads=threads)
     cpu.init(SEED)
-    t0 = time.time()
-    for ep in range(EPOCHS):
-        for p in range(LOAD):
-            cpu.present(O.load_stim(pats[p], 1.0, 1000 + p, NCOL), 10, 5, True)
-    cpu.present(O.load_stim(pats[0], 1.0, 31337, NCOL), 10, 5, True)
-    train_s = time.time() - t0
+    train_s = train(cpu, pats, O.load_stim)
+    fx = fixture()
+    planes_ok = fx is not None and trained_digest(cpu) == fx["trained_sha256_w0_w3_bias"]
     conn = cpu.read("CONN")
     ntraj = max(1, args.ref_traj)
     idx = np.linspace(0, cues.shape[0] - 1, ntraj).astype(int)
     times, evs = [], []
+    hists = []
     for it in range(args.warmup + args.steps):
-        ev = 0.0
         t1 = time.perf_counter()
         hists = []
         for b in idx:
@@ -350,17 +472,33 @@ def run_reference(args) -> None:
         if it >= args.warmup:
             times.append(dt)
             evs.append(ev)
+    match = check_against_fixture(fx, idx, hists)
+    cpu.close()
     value = float(sum(evs) / sum(times))
     line = {"impl": "reference", "metric": "synaptic events/s (batched recall, 300 trajectories x 45 steps)",
             "value": value, "unit": "synaptic events/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded cues)",
-            "config": {"workload": "batched recall, config C load 60 seed 0, 300 cues x (10 clamp + 35 free)",
+            "config": {"workload": "batched recall, config C load 60 seed 0, 300 cues (whole patterns and 10 %/25 % "
+                                   "active bits flipped) x (10 clamp + 35 free)",
                        "sample_trajectories": int(ntraj), "train_s": round(train_s, 1)},
+            "trained_planes_equal_oracle_fixture": planes_ok, "oracle_match": match,
             "cpu_baseline": {"value": value, "unit": "synaptic events/s", "cores": threads, "kind": "port",
-                             "sample": f"{ntraj} trajectories x {T_RECALL} steps per step"},
+                             "sample": f"{ntraj} of the 300 trajectories (evenly spread) x {T_RECALL} steps per step"},
             "e2e": {"value": value, "unit": "synaptic events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def time_device(net, d_cues, B, T, clamp, d_final, flush, steps) -> list[float]:
+    import torch
+
+    times = []
+    for _ in range(steps):
+        flush.zero_()  # evict L2 between timed steps (untimed: outside the device-timed launch)
+        torch.cuda.synchronize()
+        times.append(net.recall_device(d_cues.data_ptr(), B, T, clamp, d_final.data_ptr(), graph=True))
+    torch.cuda.synchronize()
+    return times
 
 
 def main() -> None:
@@ -369,13 +507,15 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="axon", choices=["axon", "reference"])
-    ap.add_argument("--ref-traj", type=int, default=6)
-    ap.add_argument("--cpu-traj", type=int, default=6)
+    ap.add_argument("--ref-traj", type=int, default=30)
+    ap.add_argument("--cpu-traj", type=int, default=120)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
     ap.add_argument("--no-multi", action="store_true", help="skip the 25-network one-launch measurement")
+    ap.add_argument("--no-pins", action="store_true", help="skip the Table 2 / high-load Table 1 networks")
     ap.add_argument("--no-serve", action="store_true", help="skip the recall-serving measurement")
+    ap.add_argument("--no-train", action="store_true", help="skip the command-line training throughput")
     ap.add_argument("--multi-nets", type=int, default=25, help="networks of the multi-network block (small cases)")
     ap.add_argument("--multi-epochs", type=int, default=EPOCHS)
     ap.add_argument("--serve-rates", default=",".join(map(str, SERVE_RATES)), help="offered loads, requests/s")
@@ -397,21 +537,25 @@ def main() -> None:
 
     if rank == 0:
         build.build_lib()
+        build.build_cli()
     rep.barrier()
     dev = torch.cuda.current_device()
-    cfg = config_c()
-    net = ax.Network(cfg, device=dev)
+    net = ax.Network(config_c(), device=dev)
     net.init(SEED)
     pats = ax.stimuli(SEED, LOAD, INCOLS, STIMCOLS)
-    train_s = train(net, pats)
-    cues = make_cues(pats)
+    train_s = train(net, pats, ax.load_stim)
+    fx = fixture()
+    planes_ok = fx is not None and trained_digest(net) == fx["trained_sha256_w0_w3_bias"]
+    cues = make_cues(pats, ax.noisy_cue, ax.noisy_cue_seed)
     B = cues.shape[0]
-    # events of the workload (fixed by the trajectories), from one recorded run
+    # events of the workload (fixed by the trajectories), from one recorded run, and every
+    # trajectory against the oracle's fixture
     ref = net.recall(cues, T_RECALL, CLAMP_RECALL, hist=True)
     conn = net.read("CONN")
     ev = events_per_step(ref["hist"], conn)
     events = float(ev.sum())
-    active_tiles = None
+    match = check_against_fixture(fx, range(B), ref["hist"])
+    match["trained_planes_equal"] = planes_ok
 
     # device-resident inputs and outputs
     d_cues = torch.from_numpy(cues.view(np.int32)).to(f"cuda:{dev}")
@@ -420,15 +564,10 @@ def main() -> None:
     for _ in range(args.warmup):  # the first call captures the launch as a CUDA graph, the rest replay it
         net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_final.data_ptr(), graph=True)
     assert np.array_equal(d_final.cpu().numpy().view(np.uint32), ref["final"])
-    times = []
     torch.cuda.synchronize()
     rep.barrier()
     with ClockSampler(dev) as clk:
-        for _ in range(args.steps):
-            flush.zero_()  # evict L2 between timed steps (untimed: outside the device-timed launch)
-            torch.cuda.synchronize()
-            times.append(net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_final.data_ptr(), graph=True))
-        torch.cuda.synchronize()
+        times = time_device(net, d_cues, B, T_RECALL, CLAMP_RECALL, d_final, flush, args.steps)
     rep.barrier()
     ms = rep.max(float(np.mean(times)))
     value = world * events / (ms / 1e3)
@@ -448,15 +587,28 @@ def main() -> None:
         assert np.array_equal(r["final"], ref["final"])
     e2e_s = rep.max(float(np.mean(e2e_t)) if e2e_t else float("nan"))
 
+    # the reference-parity variant: the wave readout's 5 clamped + 30 free steps
+    rw = net.recall(cues, T_WAVE, CLAMP_WAVE, hist=True)
+    ev_w = float(events_per_step(rw["hist"], conn).sum())
+    d_fw = torch.empty((B, NCOL), dtype=torch.int32, device=f"cuda:{dev}")
+    for _ in range(args.warmup):
+        net.recall_device(d_cues.data_ptr(), B, T_WAVE, CLAMP_WAVE, d_fw.data_ptr(), graph=True)
+    assert np.array_equal(d_fw.cpu().numpy().view(np.uint32), rw["final"])
+    tw = time_device(net, d_cues, B, T_WAVE, CLAMP_WAVE, d_fw, flush, max(5, args.steps // 2))
+    ms_w = rep.max(float(np.mean(tw)))
+    wave = {"workload": "the same 300 cues x (5 clamp + 30 free), the reference's wave readout (src/axon.mm:1804-1858)",
+            "value": world * ev_w / (ms_w / 1e3), "unit": "synaptic events/s", "ms_per_step": ms_w,
+            "events_per_batch": ev_w}
+
     # plain GPU path on the same 300 trajectories (one persistent launch per trajectory)
     plain = None
+    hbm_peak, pk = peaks()
     if not args.no_plain:
         rp = net.recall(cues, T_RECALL, CLAMP_RECALL, method="plain")
         assert np.array_equal(rp["final"], ref["final"])
         pt = [net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_final.data_ptr(), method="plain")
               for _ in range(2)]
         pms = rep.max(float(np.mean(pt)))
-        hbm_peak, pk = peaks()
         pa = plain_alg_bytes(ref["hist"], conn) / (pms / 1e3) / 1e9
         plain = {"value": world * events / (pms / 1e3), "ms_per_step": pms, "launches_per_step": B,
                  "us_per_trajectory_step": 1e3 * pms / (B * T_RECALL),
@@ -464,41 +616,46 @@ def main() -> None:
                               "peak_kind": pk, "note": "algorithmic bytes = sum over trajectory-steps of 1 KiB per "
                                                        "(column, branch) with a spiking group + conn + spikes"}}
 
-    multi = None if args.no_multi else bench_multi(dev, args.multi_nets, args.multi_epochs)
+    threads = os.cpu_count() or 1
+    ptrain = None if (args.no_train or rank != 0 or world != 1) else plain_train(dev, threads)
+    multi = None if args.no_multi else bench_multi(dev, args.multi_nets, args.multi_epochs, not args.no_pins)
     serving = None if args.no_serve else bench_serve(dev, [int(x) for x in args.serve_rates.split(",")],
                                                      args.serve_seconds, args.serve_nets)
 
     if rank != 0:
         rep.close()
         return
-    hbm, peak_kind = peaks()
-    # roofline of the batched kernel: W3 (128 MiB, read once per recall step for all
-    # trajectories) + the per-neuron u16 drive slab written every step + spike vectors
+    # roofline of the batched kernel, strict algorithmic bytes: W3 (128 MiB, read once per
+    # recall step for all trajectories) + every trajectory's spike vector read and written
+    # per step
     w3_bytes = NCOL * 32 * 1024
-    slab = B * NCOL * 32 * 2
     spikes = 2 * B * NCOL * 4
-    alg_bytes = T_RECALL * (w3_bytes + slab + spikes)
+    alg_bytes = T_RECALL * (w3_bytes + spikes)
     achieved = alg_bytes / (ms / 1e3) / 1e9
-    cpu = None if args.no_cpu else cpu_sample(cfg, net, cues, ev, os.cpu_count() or 1, args.cpu_traj)
+    cpu = None if (args.no_cpu or world != 1) else cpu_sample(net, cues, ev, ref["hist"], threads, args.cpu_traj)
     line = {
         "metric": "synaptic events/s (batched recall, 300 trajectories x 45 steps)",
         "value": value, "unit": "synaptic events/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded cues from the reference's stimulus stream)",
-        "config": {"workload": "batched recall, config C load 60 seed 0, 300 cues x (10 clamp + 35 free), bias off",
+        "config": {"workload": "batched recall, config C load 60 seed 0, 300 cues (whole patterns, and 10 %/25 % of "
+                               "their active bits flipped off, 2 draws each) x (10 clamp + 35 free), bias off",
                    "trajectories": B, "steps_per_trajectory": T_RECALL, "events_per_batch": events,
                    "train_s": round(train_s, 2), "l2": "flushed between timed steps (256 MiB write)",
                    "launch": "one persistent cooperative kernel per batch, replayed as a captured CUDA graph",
                    "parallelism": f"replicas x{world}"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": measured_traffic("k_recall"), "peak_kind": peak_kind,
-                     "note": "algorithmic bytes = 45 x (W3 128 MiB + u16 drive slab + spike vectors); the kernel is "
-                             "issue-bound, see profiles/"},
+        "oracle_match": match,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                     "traffic": measured_traffic("k_recall"), "peak_kind": pk,
+                     "note": "algorithmic bytes = 45 x (W3 128 MiB + every trajectory's spike vector in and out); "
+                             "the kernel is bound by the popcount (XU) pipe and issue, see profiles/"},
         "cpu_baseline": cpu,
         "e2e": {"value": world * events / e2e_s, "unit": "synaptic events/s", "h2d_bytes_per_step": int(cues.nbytes),
                 "d2h_bytes_per_step": int(B * NCOL * 4)},
+        "wave_variant": wave,
         "plain": plain,
         "batched_over_plain": (value / plain["value"]) if plain else None,
+        "plain_train": ptrain,
         "multi": multi,
         "serving": serving,
         "gpu_launches": args.steps,

@@ -138,6 +138,20 @@ axon_status axon_stimuli(uint32_t seed, uint32_t nstim, uint32_t incols, uint32_
 axon_status axon_load_stim(const uint32_t* cols, uint32_t ncols, double keep, uint32_t seed, uint32_t ncol,
                            uint32_t* out_ncol);
 
+/* Noisy cue: no counterpart in the reference, whose cues only drop whole pattern columns
+ * (loadStim's keep fraction, src/axon.mm:800-804). Clamp words of the whole pattern
+ * (`ncols` distinct columns, each < ncol, all 32 neurons on), then round(frac * A) of its
+ * A = 32 * ncols active bits flipped off: the active bits are listed column by column in
+ * `cols` order, bit 0 first, and the flipped ones are the first round(frac * A) picks of
+ * a forward Fisher-Yates over that list driven by mt19937(seed), pick i drawn from
+ * [i, A-1] as the shuffle of axon_stimuli draws. frac in [0, 1]. */
+axon_status axon_noisy_cue(const uint32_t* cols, uint32_t ncols, double frac, uint32_t seed, uint32_t ncol,
+                           uint32_t* out_ncol);
+/* The seed of draw `draw` of pattern q's noisy cue at `pct` percent of active bits
+ * flipped, as the CLI's cueflip row and the batched-recall benchmark use it:
+ * 90000 + 1000*pct + 16*q + draw. */
+uint32_t axon_noisy_cue_seed(uint32_t q, uint32_t pct, uint32_t draw);
+
 /* ---------------------------------------------------------------- batched readout
  * B readout trajectories of one network, each exactly what present() with learn = 0 does
  * (src/axon.mm:815-888): `cues` holds B clamp patterns of ncol words. The batched method
@@ -178,10 +192,13 @@ axon_status axon_recall_device(axon_net* net, const uint32_t* cues, uint32_t B, 
  * words, the clamp pattern). Allocates nothing - no cudaMalloc/cudaFree, no library
  * allocation: the kernel's only scratch is a fixed device array in the library sized for
  * ncol <= 4096 (about 87 KiB per GPU, held until the process exits); larger ncol returns
- * AXON_EINVAL. Runs on the default stream and returns when the presentation is done.
- * The first call on a device resolves the array's device address; make it before any
- * stream capture. Calls that overlap on the GPU share that array and race: issue one at
- * a time per device. */
+ * AXON_EINVAL. Every pointer must be 16-byte aligned (the planes are read as 16-byte
+ * vectors and W3 tiles are bulk-copied); a misaligned one returns AXON_EINVAL. The call is
+ * synchronous on the legacy default stream: it returns when the presentation is done, and
+ * must not be made while any stream of the device is being captured. The first call on a
+ * device resolves the array's device address and keeps it for the process, so the library
+ * must not outlive a cudaDeviceReset of that device. Calls that overlap on the GPU share
+ * that array and race: issue one at a time per device. */
 typedef struct axon_state_dev {
   uint32_t *w0, *w1, *w2, *w3;                   /* bitplanes (in/out) */
   uint32_t *conn, *bias, *mult, *refball, *stim; /* conn, mult, refball, stim in; bias in/out */

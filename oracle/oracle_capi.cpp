@@ -9,6 +9,7 @@
 
 #include "../include/axon_capi.h"
 #include "oracle_engine.hpp"
+#include "oracle_protocol.hpp"
 #include "oracle_rng.hpp"
 
 namespace {
@@ -158,6 +159,32 @@ void oracle_load_stim(const uint32_t* cols, uint32_t ncols, double keep, uint32_
   for (uint32_t i = 0; i < ncols; ++i)
     if (oracle::libcxx_canonical(r) <= keep) out[cols[i]] = 0xFFFFFFFFu;
 }
+// the noisy cue (see oracle::noisy_clamp) of one pattern's column list
+void oracle_noisy_cue(const uint32_t* cols, uint32_t ncols, double frac, uint32_t seed, uint32_t ncol, uint32_t* out) {
+  std::vector<uint32_t> stim(ncol);
+  oracle::noisy_clamp(std::vector<uint32_t>(cols, cols + ncols), frac, seed, stim);
+  std::copy(stim.begin(), stim.end(), out);
+}
+uint32_t oracle_noisy_seed(uint32_t q, uint32_t pct, uint32_t draw) { return oracle::noisy_seed(q, pct, draw); }
+
+// The reference's built-in defaults (src/axon.mm:688-735, restated by the oracle's own
+// key parser with no keys given) overridden by `argc` key=value strings, resolved into
+// the network configuration struct the oracle and the engine share.
+void oracle_cfg(int argc, char** argv, axon_cfg* out) {
+  std::vector<char*> av(1 + (size_t)argc);
+  static char prog[] = "axon_oracle";
+  av[0] = prog;
+  for (int i = 0; i < argc; ++i) av[1 + (size_t)i] = argv[i];
+  const oracle::Cfg c = oracle::Cfg::parse(argc + 1, av.data());
+  std::memset(out, 0, sizeof(*out));
+  out->ncol = c.NCOL; out->incols = c.IN_COLS; out->inbr = c.inBranches; out->nand = c.nAnd; out->target = c.targetC;
+  out->k = c.K; out->ktest = c.kTest; out->dthr = c.dthr; out->boost = c.boost; out->mode = c.mode;
+  out->biasup = c.biasUp; out->biasdown = c.biasDown; out->biasshift = c.biasShift;
+  out->biasdownevery = c.biasDownEvery; out->bandlo = c.bandLo; out->bandhi = c.bandHi; out->contrast = c.contrast;
+  out->margingate = c.margGate; out->hetero = c.hetero; out->ltdrep = c.ltdRep; out->ltdevery = c.ltdEvery;
+  out->facil = c.facil; out->topkpar = c.topkPar;
+}
+
 // raw draws of the restated distributions, for known-answer checks
 void oracle_uniform_int(uint32_t seed, uint64_t a, uint64_t b, uint32_t n, uint64_t* out) {
   std::mt19937 r(seed);

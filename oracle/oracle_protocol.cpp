@@ -379,10 +379,15 @@ int Protocol::run() {
 
     printf("\n  pattern completion with bias OFF at test  (keep=0 is the no-cue control)\n");
     printf("  cue  |  vs CLAMPED ref(biasON): self  other  margin | vs noBias ref: self  other  margin\n");
-    for (double keep : {1.0, 0.75, 0.5, 0.35, 0.25, 0.15, 0.10, 0.05, 0.02, 0.0}) {
+    // cueflip=P adds an 11th row (no counterpart in the reference): keep = -P/100 marks the
+    // whole pattern with P% of its active bits flipped off (noisy_clamp, draw 0)
+    std::vector<double> rows = {1.0, 0.75, 0.5, 0.35, 0.25, 0.15, 0.10, 0.05, 0.02, 0.0};
+    if (C.cueflip) rows.push_back(-(double)C.cueflip / 100.0);
+    for (double keep : rows) {
       double s1 = 0, o1 = 0, s2 = 0, o2 = 0;
       for (uint32_t q = 0; q < NSTIM; ++q) {
-        present(q, keep, T, CLAMP, false, true, 4400 + q, 0u);
+        if (keep < 0) present_noisy(q, -keep, T, CLAMP, noisy_seed(q, C.cueflip, 0));
+        else present(q, keep, T, CLAMP, false, true, 4400 + q, 0u);
         Cols a = assemblyOf(T);
         s1 += overlap(a, refClampCols[q]);
         s2 += overlap(a, refNBCols[q]);
@@ -391,8 +396,12 @@ int Protocol::run() {
           if (r != q) { b1 = std::max(b1, overlap(a, refClampCols[r])); b2 = std::max(b2, overlap(a, refNBCols[r])); }
         o1 += b1; o2 += b2;
       }
-      printf("  %3.0f%% |%25.3f %6.3f %+7.3f |%18.3f %6.3f %+7.3f\n", keep * 100, s1 / NSTIM, o1 / NSTIM,
-             s1 / NSTIM - o1 / NSTIM, s2 / NSTIM, o2 / NSTIM, s2 / NSTIM - o2 / NSTIM);
+      if (keep >= 0)
+        printf("  %3.0f%% |%25.3f %6.3f %+7.3f |%18.3f %6.3f %+7.3f\n", keep * 100, s1 / NSTIM, o1 / NSTIM,
+               s1 / NSTIM - o1 / NSTIM, s2 / NSTIM, o2 / NSTIM, s2 / NSTIM - o2 / NSTIM);
+      else
+        printf("  flip%3u%% |%21.3f %6.3f %+7.3f |%18.3f %6.3f %+7.3f\n", C.cueflip, s1 / NSTIM, o1 / NSTIM,
+               s1 / NSTIM - o1 / NSTIM, s2 / NSTIM, o2 / NSTIM, s2 / NSTIM - o2 / NSTIM);
     }
     printf("======================================================================\n");
   }

@@ -34,7 +34,7 @@ struct Cfg {
   uint32_t nAnd, targetC, K, dthr, boost, mode, EPOCHS, T, CLAMP, NSTIM, quiet, seed, split,
       unionchar, biasUp, biasDown, biasShift, biasDownEvery, inBranches, STIM_COLS, IN_COLS,
       NCOL, diag, profile, topkPar, vtopk, contrast, bandLo, bandHi, margGate, hetero, vbs,
-      ltdRep, ltdEvery, kTest, facil, deep, wave, waveT, trainClamp;
+      ltdRep, ltdEvery, kTest, facil, deep, wave, waveT, trainClamp, cueflip;
   static Cfg parse(int argc, char** argv) {
     Cfg c;
     c.nAnd = argu(argc, argv, "nand", 4);
@@ -76,6 +76,7 @@ struct Cfg {
     c.deep = argu(argc, argv, "deep", 0);
     c.wave = argu(argc, argv, "wave", 0);
     c.waveT = argu(argc, argv, "wavet", 35);
+    c.cueflip = argu(argc, argv, "cueflip", 0);  // not a reference key: noisy-cue recall row
     c.trainClamp = argu(argc, argv, "trainclamp", c.contrast ? c.CLAMP : c.T);
     if (c.biasUp == 1u) {  // "auto" (src/axon.mm:732-735)
       double pr = (double)c.targetC * c.K / (double)(c.NCOL - c.IN_COLS) / NPC;
@@ -94,6 +95,7 @@ struct Cfg {
     if (T == 0 || T > MAXT) return "T must be in 1..64";
     if (STIM_COLS > IN_COLS) return "stimcols must be <= incols";
     if (NSTIM == 0) return "stim must be >= 1";
+    if (cueflip > 100) return "cueflip must be a percentage in 0..100";
     return "";
   }
 };
@@ -153,6 +155,20 @@ class Protocol {
     std::mt19937 r(sd);
     for (uint32_t c : stimCols[p])
       if (libcxx_canonical(r) <= keep) E.stim[c] = 0xFFFFFFFFu;
+  }
+
+  // a readout presentation from a noisy cue (noisy_clamp) instead of loadStim; otherwise
+  // present(..., learn = false, freeze = true, useBias = 0)
+  void present_noisy(uint32_t p, double frac, uint32_t T_, uint32_t clampSteps, uint32_t sd) {
+    P.k = (C.kTest != 0u) ? C.kTest : C.K;
+    P.facil = C.facil;
+    P.useBias = 0u;
+    noisy_clamp(stimCols[p], frac, sd, E.stim);
+    std::fill(E.stats.begin(), E.stats.end(), 0u);
+    P.histOn = 1u;
+    std::fill(E.spk[0].begin(), E.spk[0].end(), 0u);
+    std::fill(E.spk[1].begin(), E.spk[1].end(), 0u);
+    for (uint32_t t = 0; t < T_; ++t) step(t, clampSteps, false, true);
   }
 
   // present(), src/axon.mm:815-888; returns wall ms per step

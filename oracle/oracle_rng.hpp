@@ -45,4 +45,26 @@ inline double libcxx_canonical(std::mt19937& g) {
   return s / 18446744073709551616.0;
 }
 
+// Noisy cue (no counterpart in the reference; the engine's axon_noisy_cue is the product
+// side): start from the whole pattern clamped on, enumerate its active bits as
+// (pattern position p, bit b) -> 32 p + b, and switch off the first round(frac * A)
+// elements of a forward Fisher-Yates permutation of 0..A-1 drawn with
+// libcxx_uniform_int(g, i, A-1) from mt19937(seed).
+inline void noisy_clamp(const std::vector<uint32_t>& cols, double frac, uint32_t seed, std::vector<uint32_t>& stim) {
+  std::fill(stim.begin(), stim.end(), 0u);
+  for (uint32_t c : cols) stim[c] = 0xFFFFFFFFu;
+  const uint64_t A = 32ull * cols.size();
+  uint64_t k = (uint64_t)(frac * (double)A + 0.5);
+  if (k > A) k = A;
+  std::vector<uint64_t> perm(A);
+  for (uint64_t i = 0; i < A; ++i) perm[i] = i;
+  std::mt19937 g(seed);
+  for (uint64_t i = 0; i < k; ++i) {
+    std::swap(perm[i], perm[libcxx_uniform_int(g, i, A - 1)]);
+    stim[cols[perm[i] / 32]] &= ~(1u << (perm[i] % 32));
+  }
+}
+
+inline uint32_t noisy_seed(uint32_t q, uint32_t pct, uint32_t draw) { return 90000u + 1000u * pct + 16u * q + draw; }
+
 }  // namespace oracle

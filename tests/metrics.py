@@ -45,3 +45,18 @@ def scrape(out: str) -> dict:
             m["steps_per_s"] = g.group(1)
             break
     return m
+
+
+def seeds_summary(per_seed: list[dict]) -> dict:
+    """Five-seed summary as the reference's bench/seeds.sh computes it: each seed's
+    sustained ratio (printed with %.3f), margin and within-assembly density as printed;
+    mean and sample standard deviation of each, printed with the script's formats."""
+    import statistics as st
+
+    v = [float(m["sustained"]) for m in per_seed]
+    mg = [float(m["margin"]) for m in per_seed]
+    d = [float(m["within_pct"]) for m in per_seed]
+    return {"sustained_mean": f"{st.mean(v):.3f}", "sustained_sd": f"{st.stdev(v):.3f}",
+            "margin_mean": f"{st.mean(mg):+.3f}", "margin_sd": f"{st.stdev(mg):.3f}",
+            "within_mean": f"{st.mean(d):.2f}", "within_sd": f"{st.stdev(d):.2f}",
+            "sustained_cv_pct": f"{100 * st.stdev(v) / st.mean(v):.1f}"}

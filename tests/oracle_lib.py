@@ -23,7 +23,27 @@ BUF = {
     "STATS": 16, "HIST": 17, "THETA": 18,
 }
 
+CFG_FIELDS = [
+    "ncol", "incols", "inbr", "nand", "target", "k", "ktest", "dthr", "boost", "mode", "biasup",
+    "biasdown", "biasshift", "biasdownevery", "bandlo", "bandhi", "contrast", "margingate", "hetero",
+    "ltdrep", "ltdevery", "facil", "topkpar",
+]
+
+
+class OracleCfg(C.Structure):
+    """The network configuration struct of include/axon_capi.h, declared here so that the
+    oracle can be driven without loading the engine library."""
+    _fields_ = [(f, C.c_uint32) for f in CFG_FIELDS] + [("reserved", C.c_uint32 * 9)]
+
+
 _lib = None
+
+
+def default_threads() -> int:
+    """Host threads for an oracle run: AXON_ORACLE_THREADS, else every core."""
+    import os
+
+    return int(os.environ.get("AXON_ORACLE_THREADS", "0")) or (os.cpu_count() or 1)
 
 
 def build() -> None:
@@ -55,6 +75,10 @@ def load():
         L.oracle_load_stim.argtypes = [U32P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, U32P]
         L.oracle_uniform_int.argtypes = [C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_uint64)]
         L.oracle_canonical.argtypes = [C.c_uint32, C.c_uint32, C.POINTER(C.c_double)]
+        L.oracle_noisy_cue.argtypes = [U32P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, U32P]
+        L.oracle_noisy_seed.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
+        L.oracle_noisy_seed.restype = C.c_uint32
+        L.oracle_cfg.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.c_void_p]
         _lib = L
     return _lib
 
@@ -125,6 +149,28 @@ class OracleNet:
         self.L.oracle_wdiag(self._h, u32(np.ascontiguousarray(memb, dtype=np.uint32)),
                             u32(np.ascontiguousarray(asm_spk, dtype=np.uint32)), nstim, sel, u32(out))
         return out
+
+
+def config(**kw) -> OracleCfg:
+    """The reference's built-in defaults as the oracle's own key parser restates them
+    (src/axon.mm:688-735), with CLI keys overridden by ``kw`` (key=value, as on the command
+    line; e.g. config(ncol=4096, target=64))."""
+    args = [f"{k}={int(v)}".encode() for k, v in kw.items()]
+    argv = (C.c_char_p * max(1, len(args)))(*args)
+    c = OracleCfg()
+    load().oracle_cfg(len(args), argv, C.byref(c))
+    return c
+
+
+def noisy_cue(cols, frac, seed, ncol) -> np.ndarray:
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    out = np.empty(ncol, dtype=np.uint32)
+    load().oracle_noisy_cue(u32(cols), cols.size, frac, seed, ncol, u32(out))
+    return out
+
+
+def noisy_seed(q, pct, draw) -> int:
+    return int(load().oracle_noisy_seed(q, pct, draw))
 
 
 def stimuli(seed, nstim, incols, stimcols) -> np.ndarray:

@@ -63,3 +63,50 @@ def test_bad_config_is_an_error_not_an_exit(capi):
         ax.Network(ax.config(ncol=100))  # not a multiple of 32
     with pytest.raises(AxonError):
         ax.Network(ax.config(ncol=256, incols=256))
+
+
+@pytest.mark.parametrize("frac", [0.0, 0.10, 0.25, 0.5, 1.0])
+def test_noisy_cue_matches_oracle(capi, frac):
+    """axon_noisy_cue against the oracle's own restatement, and its defining properties:
+    only active bits are flipped, exactly round(frac * 32 * ncols) of them, and a smaller
+    fraction flips a subset of a larger one's bits for the same seed."""
+    import axon_b200 as ax
+
+    pats = O.stimuli(0, 60, 512, 64)
+    for q in (0, 17, 59):
+        for pct, d in ((10, 0), (10, 1), (25, 0), (25, 1)):
+            sd = ax.noisy_cue_seed(q, pct, d)
+            assert sd == O.noisy_seed(q, pct, d) == 90000 + 1000 * pct + 16 * q + d
+            got = ax.noisy_cue(pats[q], frac, sd, 4096)
+            assert np.array_equal(got, O.noisy_cue(pats[q], frac, sd, 4096))
+            full = ax.clamp_words(pats[q], 4096)
+            assert np.all(got & ~full == 0)  # only active bits change
+            flipped = int(np.bitwise_count(full).sum() - np.bitwise_count(got).sum())
+            assert flipped == int(np.floor(frac * 64 * 32 + 0.5))
+            if frac < 1.0:
+                more = ax.noisy_cue(pats[q], min(1.0, frac + 0.25), sd, 4096)
+                assert np.all(more & ~got == 0)  # the larger fraction's flips include these
+
+
+def test_noisy_cue_rejects_bad_input(capi):
+    import axon_b200 as ax
+    from axon_b200._capi import AxonError
+
+    with pytest.raises(AxonError):
+        ax.noisy_cue(np.array([3, 3], dtype=np.uint32), 0.1, 1, 64)  # repeated column
+    with pytest.raises(AxonError):
+        ax.noisy_cue(np.array([70], dtype=np.uint32), 0.1, 1, 64)  # column out of range
+    with pytest.raises(AxonError):
+        ax.noisy_cue(np.array([1], dtype=np.uint32), 1.5, 1, 64)  # fraction above 1
+
+
+def test_oracle_config_defaults_match_engine_defaults(capi):
+    """The oracle's restated CLI defaults and the engine's axon_cfg_defaults agree field for
+    field, with and without overrides (the reference arm builds its configuration from the
+    oracle's alone)."""
+    import axon_b200 as ax
+
+    for kw in ({}, dict(ncol=4096, incols=512, **ax.CONFIG_C)):
+        o, e = O.config(**kw), ax.config(**kw)
+        for f in O.CFG_FIELDS:
+            assert getattr(o, f) == getattr(e, f), f

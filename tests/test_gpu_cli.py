@@ -53,6 +53,8 @@ def assert_same(args):
     [*CONFIG_C, "stim=3", "epochs=0", "deep=1", "margingate=1", "hetero=1", "seed=9"],
     [*CONFIG_C, "stim=7", "epochs=1", "T=20", "clampsteps=8", "trainclamp=6", "mode=0", "dthr=3", "wave=1",
      "wavet=60", "biasdownevery=3"],
+    [*CONFIG_C, "stim=6", "epochs=3", "cueflip=25"],                  # the noisy-cue recall row (not a reference key)
+    [*CONFIG_C, "stim=5", "epochs=2", "cueflip=10", "T=12"],
 ])
 def test_cli_matches_oracle_small(extra):
     assert_same([*SMALL, *extra])

@@ -33,15 +33,20 @@ def device_copy(net):
     return bufs
 
 
-def static_present(cfg, bufs, stim, T, clamp, learn, use_bias):
+def static_present(cfg, bufs, stim, T, clamp, learn, use_bias) -> int:
+    """One call through the C ABI; returns the change in free device memory across it."""
     import torch
 
     from axon_b200 import _capi as A
 
     bufs["stim"].copy_(torch.from_numpy(np.ascontiguousarray(stim, dtype=np.uint32).view(np.int32)))
     st = A.StateDev(**{f: C.c_void_p(bufs[f].data_ptr()) for f in NAMES})
-    A.check(A.lib().axon_present_static(C.byref(cfg), C.byref(st), T, clamp, int(learn), use_bias))
     torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    A.check(A.lib().axon_present_static(C.byref(cfg), C.byref(st), T, clamp, int(learn), use_bias))
+    free1 = torch.cuda.mem_get_info()[0]
+    torch.cuda.synchronize()
+    return free1 - free0
 
 
 @pytest.mark.parametrize("geometry", ["small", "full"])
@@ -64,7 +69,9 @@ def test_static_present_matches_present(geometry):
              (ax.load_stim(pats[3], 0.75, 4403, cfg.ncol), 35, 5, False, 0)]
     for i, (stim, T, clamp, learn, ub) in enumerate(calls):
         net.present(stim, T, clamp, learn, True, ub)
-        static_present(cfg, bufs, stim, T, clamp, learn, ub)
+        delta = static_present(cfg, bufs, stim, T, clamp, learn, ub)
+        if i > 0:  # the first call on the device may load the module; later calls allocate nothing
+            assert delta == 0, f"call {i}: free device memory changed by {delta} bytes"
         for name in COMPARE + ["HIST", "THETA"]:
             field = next(f for f, n in NAMES.items() if n == name)
             got = bufs[field].cpu().numpy().view(np.uint32)
@@ -85,3 +92,21 @@ def test_static_present_rejects_oversized_network():
     status = A.lib().axon_present_static(C.byref(cfg), C.byref(st), 10, 5, 0, 0)
     assert status == A.AXON_EINVAL
     assert b"4096" in A.lib().axon_last_error()
+
+
+def test_static_present_rejects_misaligned_pointer():
+    """The planes are read as 16-byte vectors and W3 tiles are bulk-copied, so a pointer
+    that is not 16-byte aligned is refused before anything is launched."""
+    import torch
+
+    import axon_b200 as ax
+    from axon_b200 import _capi as A
+
+    cfg = ax.config(**dict(ax.CONFIG_C, ncol=256, incols=64, target=16, k=12))
+    buf = torch.zeros(64, dtype=torch.int32, device="cuda")
+    ptrs = {f: C.c_void_p(buf.data_ptr()) for f in NAMES}
+    ptrs["w3"] = C.c_void_p(buf.data_ptr() + 4)  # never dereferenced: rejected first
+    st = A.StateDev(**ptrs)
+    status = A.lib().axon_present_static(C.byref(cfg), C.byref(st), 10, 5, 0, 0)
+    assert status == A.AXON_EINVAL
+    assert b"16-byte aligned" in A.lib().axon_last_error()
