@@ -46,7 +46,106 @@ cudaError_t launch_make_w3r(const uint4* W3, uint32_t* W3R, uint32_t ncol, cudaS
   return cudaGetLastError();
 }
 
+// One m16n8k256 binary MMA: d = c + popcount(a AND b) over 256 bits, a 16 x 256 bit rows
+// (row-major fragment), b 256 x 8 bit columns, c/d 16 x 8 int32.
+__device__ __forceinline__ void mma_b1_and(uint32_t (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k256.row.col.s32.b1.b1.s32.and.popc {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Phase-1 entry units of one work item on the tensor cores. A unit is a chunk of 8 entries
+// of one branch (the branch's single-word entries first, then its multi-word ones); the
+// warp's lanes hold the fragments of m16n8k256: lane = 4 * g + q holds rows g, g+8 (and
+// g+16, g+24 in the second MMA) of the tile at 32-bit words q and q+4, and entry g's spike
+// words q and q+4. The counts come back as rows g, g+8 for entries 2q, 2q+1; each count
+// becomes its dendritic term and is added into the entry's trajectory row, packed in pairs
+// of rows with the lane that holds the neighbouring row (lane ^ 4).
 template <bool PACK, bool LIN>
+__device__ __forceinline__ void mma_units(const uint32_t* cPC, const uint32_t* cP1, const uint32_t* cPM,
+                                          const uint32_t* cConn, const uint32_t* tileBase, uint32_t* accB,
+                                          uint32_t accStride, uint32_t* unitCtr, const uint2* e1In, const uint4* eMIn,
+                                          const uint32_t* spkIn, uint32_t B, uint32_t ncol, uint32_t dthr,
+                                          uint32_t bst, uint32_t lane) {
+  const uint32_t nchunks = cPC[64];
+  const uint32_t g4 = lane >> 2, q = lane & 3u;
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  for (;;) {
+    uint32_t u = 0;
+    if (lane == 0) u = atomicAdd(unitCtr, 1u);
+    u = __shfl_sync(kFull, u, 0);
+    if (u >= nchunks) break;
+    // the chunk's branch: how many branches end at or before chunk u
+    const uint32_t sp = (uint32_t)__popc(__ballot_sync(kFull, cPC[lane + 1] <= u)) +
+                        (uint32_t)__popc(__ballot_sync(kFull, cPC[lane + 33] <= u));
+    const uint32_t G = cConn[sp];
+    const uint32_t n1 = cP1[sp + 1] - cP1[sp], nE = n1 + (cPM[sp + 1] - cPM[sp]);
+    const uint32_t e = 8u * (u - cPC[sp]) + g4;
+    uint32_t bq = kNone, b0 = 0u, b1 = 0u;
+    if (e < n1) {
+      const uint2 en = __ldcg(e1In + (size_t)G * B + e);
+      const uint32_t w = en.x >> 16;
+      bq = en.x & 0xFFFFu;
+      b0 = w == q ? en.y : 0u;
+      b1 = w == q + 4u ? en.y : 0u;
+    } else if (e < nE) {
+      const uint4 en = __ldcg(eMIn + (size_t)G * B + (e - n1));
+      const uint32_t nz = (en.x >> 16) & 0xFFu;
+      bq = en.x & 0xFFFFu;
+      const uint32_t* sw = spkIn + (size_t)bq * ncol + 8u * G;
+      b0 = ((nz >> q) & 1u) ? __ldcg(sw + q) : 0u;
+      b1 = ((nz >> (q + 4u)) & 1u) ? __ldcg(sw + q + 4u) : 0u;
+    }
+    const uint32_t* tile = tileBase + (sp >> 5) * kColWords + (sp & 31u) * 256u;
+    uint32_t a[4], a2[4], c0[4] = {0u, 0u, 0u, 0u}, c1[4] = {0u, 0u, 0u, 0u};
+    a[0] = tile[w3r_pos(g4, q)];
+    a[1] = tile[w3r_pos(g4 + 8u, q)];
+    a[2] = tile[w3r_pos(g4, q + 4u)];
+    a[3] = tile[w3r_pos(g4 + 8u, q + 4u)];
+    a2[0] = tile[w3r_pos(g4 + 16u, q)];
+    a2[1] = tile[w3r_pos(g4 + 24u, q)];
+    a2[2] = tile[w3r_pos(g4 + 16u, q + 4u)];
+    a2[3] = tile[w3r_pos(g4 + 24u, q + 4u)];
+    __syncwarp();
+    mma_b1_and(c0, a, b0, b1);
+    mma_b1_and(c1, a2, b0, b1);
+    // the trajectories of entries 2q and 2q+1 (held by lanes 8q and 8q + 4)
+    const uint32_t bA = __shfl_sync(kFull, bq, 8u * q), bB = __shfl_sync(kFull, bq, 8u * q + 4u);
+    // terms by row block k (rows g4 + 8k): tA for entry 2q, tB for entry 2q+1
+    uint32_t tA[4], tB[4];
+    tA[0] = branch_term<LIN>(c0[0], dthr, bst); tB[0] = branch_term<LIN>(c0[1], dthr, bst);
+    tA[1] = branch_term<LIN>(c0[2], dthr, bst); tB[1] = branch_term<LIN>(c0[3], dthr, bst);
+    tA[2] = branch_term<LIN>(c1[0], dthr, bst); tB[2] = branch_term<LIN>(c1[1], dthr, bst);
+    tA[3] = branch_term<LIN>(c1[2], dthr, bst); tB[3] = branch_term<LIN>(c1[3], dthr, bst);
+    uint32_t* rowA = bA != kNone ? accB + ((sp >> 5) * B + bA) * accStride : nullptr;
+    uint32_t* rowB = bB != kNone ? accB + ((sp >> 5) * B + bB) * accStride : nullptr;
+    if (PACK) {
+      // rows g4 and g4 ^ 1 share a counter word: the even lane adds entry 2q's pair, the odd
+      // lane entry 2q+1's
+      const bool ev = (g4 & 1u) == 0u;
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k) {
+        const uint32_t x = __shfl_xor_sync(kFull, ev ? tB[k] : tA[k], 4);
+        const uint32_t pr = ((g4 & ~1u) + 8u * k) >> 1;
+        if (ev) { if (rowA) atomicAdd(rowA + pr, tA[k] | (x << 16)); }
+        else if (rowB) atomicAdd(rowB + pr, x | (tB[k] << 16));
+      }
+    } else {
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k) {
+        if (rowA) atomicAdd(rowA + g4 + 8u * k, tA[k]);
+        if (rowB) atomicAdd(rowB + g4 + 8u * k, tB[k]);
+      }
+    }
+  }
+}
+
+// MMA: the AND-popcount contraction of phase 1 on the tensor cores (mma.sync b1 and.popc,
+// m16n8k256: 16 tile rows x 8 entries x the group's 256 spike bits per instruction) instead
+// of __popc on the CUDA cores; the dendritic terms, counters and everything else are shared.
+template <bool PACK, bool LIN, bool MMA>
 __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   extern __shared__ __align__(128) uint32_t sm[];
   const uint32_t ncol = c.ncol, incols = c.incols, B = c.B, ngrp = ncol / 8u;
@@ -58,7 +157,8 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   uint32_t* sConn = sAcc + (c.dacc ? 2u : 1u) * accWords;  // [2][64] groups of the item's branches
   uint32_t* sP1 = sConn + 2 * 64;                        // [2][68] single-word entries: prefix over 64 branches
   uint32_t* sPM = sP1 + 2 * 68;                          // [2][68] multi-word entries
-  uint32_t* sMisc = sPM + 2 * 68;  // [16]: grid barrier flag, first item, -, -, gated count, -, unit counters [2], next items [2]
+  uint32_t* sPC = sPM + 2 * 68;                          // [2][68] MMA: chunks of 8 entries, prefix over branches
+  uint32_t* sMisc = sPC + 2 * 68;  // [16]: grid barrier flag, first item, -, -, gated count, -, unit counters [2], next items [2]
   uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
   // phase-2 views reuse the tile buffers; a second drive buffer follows them when it fits
   uint32_t* sSpk = sTile + ncol;
@@ -98,11 +198,23 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     sConn[buf * 64u + 32u + lane] = g1;
     uint32_t a0 = __ldcg(c1In + g0), a1 = v1 ? __ldcg(c1In + g1) : 0u;
     uint32_t m0 = __ldcg(cMIn + g0), m1 = v1 ? __ldcg(cMIn + g1) : 0u;
+    uint32_t k0 = (a0 + m0 + 7u) >> 3, k1 = (a1 + m1 + 7u) >> 3;  // MMA chunks of the branch
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
       const uint32_t x0 = __shfl_up_sync(kFull, a0, off), x1 = __shfl_up_sync(kFull, a1, off);
       const uint32_t y0 = __shfl_up_sync(kFull, m0, off), y1 = __shfl_up_sync(kFull, m1, off);
       if (lane >= (uint32_t)off) { a0 += x0; a1 += x1; m0 += y0; m1 += y1; }
+      if (MMA) {
+        const uint32_t z0 = __shfl_up_sync(kFull, k0, off), z1 = __shfl_up_sync(kFull, k1, off);
+        if (lane >= (uint32_t)off) { k0 += z0; k1 += z1; }
+      }
+    }
+    if (MMA) {
+      const uint32_t totK = __shfl_sync(kFull, k0, 31);
+      uint32_t* PC = sPC + buf * 68u;
+      PC[1 + lane] = k0;
+      PC[33 + lane] = totK + k1;
+      if (lane == 0) PC[0] = 0u;
     }
     const uint32_t totA = __shfl_sync(kFull, a0, 31), totM = __shfl_sync(kFull, m0, 31);
     uint32_t* P1 = sP1 + buf * 68u;
@@ -185,6 +297,10 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       // last are single-word ones
       const uint32_t E1 = cP1[64], EM = cPM[64], E = E1 + EM, units = (E + 31u) >> 5;
       const uint32_t* tileBase = sTile + bcur * kItemWords;
+      if (MMA) {
+        mma_units<PACK, LIN>(sPC + bcur * 68u, cP1, cPM, cConn, tileBase, accB, accStride, sMisc + 6 + bcur, e1In,
+                             eMIn, spkIn, B, ncol, dthr, bst, lane);
+      } else
       for (;;) {
         uint32_t u = 0;
         if (lane == 0) u = atomicAdd(sMisc + 6 + bcur, 1u);
@@ -422,28 +538,34 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
 size_t recall_smem_bytes(uint32_t ncol, uint32_t B, uint32_t acc32, uint32_t dacc) {
   (void)ncol;
   const size_t stride = acc32 ? 33 : 17;
-  return (2ull * kItemWords + (dacc ? 2 : 1) * kRecallCpi * (size_t)B * stride + 2 * (64 + 68 + 68) + 16 + 4) * 4;
+  return (2ull * kItemWords + (dacc ? 2 : 1) * kRecallCpi * (size_t)B * stride + 2 * (64 + 68 + 68 + 68) + 16 + 4) * 4;
 }
 
 namespace {
-const void* recall_fn(uint32_t acc32, uint32_t lin) {
-  if (acc32) return lin ? (const void*)k_recall<false, true> : (const void*)k_recall<false, false>;
-  return lin ? (const void*)k_recall<true, true> : (const void*)k_recall<true, false>;
+template <bool PACK, bool LIN>
+const void* recall_fn_m(uint32_t mma) {
+  return mma ? (const void*)k_recall<PACK, LIN, true> : (const void*)k_recall<PACK, LIN, false>;
+}
+const void* recall_fn(uint32_t acc32, uint32_t lin, uint32_t mma) {
+  if (acc32) return lin ? recall_fn_m<false, true>(mma) : recall_fn_m<false, false>(mma);
+  return lin ? recall_fn_m<true, true>(mma) : recall_fn_m<true, false>(mma);
 }
 }  // namespace
 
 cudaError_t recall_max_blocks_per_sm(int acc32, int threads, size_t smem, int* out) {
-  for (uint32_t lin = 0; lin < 2; ++lin) {
-    cudaError_t e = cudaFuncSetAttribute(recall_fn(acc32, lin), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, recall_fn(acc32, 1), threads, smem);
+  for (uint32_t lin = 0; lin < 2; ++lin)
+    for (uint32_t mma = 0; mma < 2; ++mma) {
+      cudaError_t e = cudaFuncSetAttribute(recall_fn(acc32, lin, mma), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, recall_fn(acc32, 1, 0), threads, smem);
 }
 
 cudaError_t launch_recall(const RecallDev& d, const RecallCfg& c, const RecallShape& s, cudaStream_t st) {
   void* args[] = {(void*)&d, (void*)&c};
-  return cudaLaunchCooperativeKernel(recall_fn(c.acc32, c.mode != 2u), dim3(s.grid), dim3(s.threads), args, s.smem,
-                                     st);
+  return cudaLaunchCooperativeKernel(recall_fn(c.acc32, c.mode != 2u, c.mma), dim3(s.grid), dim3(s.threads), args,
+                                     s.smem, st);
 }
 
 }  // namespace axon

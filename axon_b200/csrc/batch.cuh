@@ -39,6 +39,7 @@ struct RecallCfg {
   uint32_t acc32;  // 1: per-neuron drive kept as u32 (packing two 16-bit sums would overflow)
   uint32_t bst;    // dendritic bonus per branch at or above dthr: boost (mode 1), 0 (mode 0)
   uint32_t dacc;   // 1: two counter buffers (alternating items), when they fit in shared memory
+  uint32_t mma;    // 1: phase-1 AND-popcounts on the tensor cores (binary MMA), 0: __popc on the CUDA cores
   uint64_t waitNs;
 };
 

@@ -57,7 +57,8 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
   if (!initialized) return set_error(AXON_ESTATE, "recall before init");
   if (B == 0) return set_error(AXON_EINVAL, "B must be >= 1");
   if (a.T == 0 || a.T > 64) return set_error(AXON_EINVAL, "T must be in 1..64");
-  if (a.use_bias > 1 || a.method > 1) return set_error(AXON_EINVAL, "bad use_bias or method");
+  if (a.use_bias > 1 || a.method > 1 || a.contraction > 1)
+    return set_error(AXON_EINVAL, "bad use_bias, method or contraction");
   CK(cudaSetDevice(device));
 
   // ---- device views of the caller's arrays (copied in when they are host arrays)
@@ -129,6 +130,7 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     const uint64_t maxAcc = (cfg.mode == 2 ? 32ull : 32ull * (256ull + cfg.boost)) + cfg.facil;
     rc.acc32 = maxAcc > 65535ull ? 1u : 0u;
     rc.bst = cfg.mode == 1 ? cfg.boost : 0u;
+    rc.mma = a.contraction == AXON_CONTRACT_TENSOR ? 1u : 0u;
     const uint32_t maxB = rc.acc32 ? 300u : kRecallMaxB;
     const uint32_t Bc = std::min(B, maxB);  // trajectories per launch
     const size_t bnc = (size_t)Bc * ncol;
@@ -166,7 +168,7 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     // everything the launches depend on: a captured graph is replayed only for the same key
     const std::vector<uint64_t> key = {(uint64_t)dCues, (uint64_t)dRef, (uint64_t)dFinal, (uint64_t)dHist,
                                        (uint64_t)dStats, (uint64_t)dLog, (uint64_t)scratch.p, (uint64_t)w3b, B, a.T,
-                                       a.clamp_steps, a.use_bias, (uint64_t)rs.grid, wait_ns};
+                                       a.clamp_steps, a.use_bias, (uint64_t)rs.grid, wait_ns, a.contraction};
     const bool graph = a.graph != 0u;
     const bool replay = graph && recallGraph && key == recallKey;
     if (graph && !replay) {

@@ -117,8 +117,12 @@ class Network:
 
     def recall(self, cues: np.ndarray, T: int, clamp_steps: int, use_bias: int = 0, method: str = "batched",
                hist: bool = False, stats: bool = False, ref_ball: np.ndarray | None = None,
-               drive_log: np.ndarray | None = None, graph: bool = False, final_out: np.ndarray | None = None) -> dict:
+               drive_log: np.ndarray | None = None, graph: bool = False, final_out: np.ndarray | None = None,
+               contraction: str = "popc") -> dict:
         """B readout trajectories (present() with learn=0 for each cue row) in one call.
+
+        contraction: "popc" (CUDA cores) or "tensor" (binary MMA) computes the batched
+        method's AND-popcounts; the results are the same.
 
         Returns {"final": (B, ncol), "hist": (B, T, ncol) | None, "stats": (B, 1024) | None,
         "drive_log": (B, 256) | None, "gpu_ms": float}. final_out, a C-contiguous uint32
@@ -129,7 +133,8 @@ class Network:
         B = cues.shape[0]
         assert cues.shape == (B, self.ncol)
         a = A.RecallArgs(T=T, clamp_steps=clamp_steps, use_bias=use_bias,
-                         method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN, graph=int(graph))
+                         method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN, graph=int(graph),
+                         contraction=A.CONTRACT_TENSOR if contraction == "tensor" else A.CONTRACT_POPC)
         if final_out is not None:
             assert final_out.dtype == np.uint32 and final_out.shape == (B, self.ncol) and final_out.flags.c_contiguous
         out = {"final": final_out if final_out is not None else np.empty((B, self.ncol), dtype=np.uint32),
@@ -151,11 +156,13 @@ class Network:
         return out
 
     def recall_device(self, cues_ptr: int, B: int, T: int, clamp_steps: int, final_ptr: int | None = None,
-                      use_bias: int = 0, method: str = "batched", graph: bool = False) -> float:
+                      use_bias: int = 0, method: str = "batched", graph: bool = False,
+                      contraction: str = "popc") -> float:
         """Device-resident variant: cues/final are device addresses on this network's GPU.
         graph=True replays a captured CUDA graph of the launch while the arguments repeat."""
         a = A.RecallArgs(T=T, clamp_steps=clamp_steps, use_bias=use_bias,
-                         method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN, graph=int(graph))
+                         method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN, graph=int(graph),
+                         contraction=A.CONTRACT_TENSOR if contraction == "tensor" else A.CONTRACT_POPC)
         ms = C.c_double()
         A.check(A.lib().axon_recall_device(self._h, C.c_void_p(cues_ptr), B, C.byref(a), None,
                                            None if final_ptr is None else C.c_void_p(final_ptr), None, None, None,

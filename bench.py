@@ -600,6 +600,24 @@ def main() -> None:
             "value": world * ev_w / (ms_w / 1e3), "unit": "synaptic events/s", "ms_per_step": ms_w,
             "events_per_batch": ev_w}
 
+    # A/B of the contraction unit: the same batch with k_drive's AND-popcounts on the tensor
+    # cores (binary MMA, m16n8k256 and.popc) instead of __popc on the CUDA cores
+    rt = net.recall(cues, T_RECALL, CLAMP_RECALL, hist=True, contraction="tensor")
+    tensor_exact = bool(np.array_equal(rt["hist"], ref["hist"]))
+    for _ in range(args.warmup):
+        net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_fw.data_ptr(), graph=True, contraction="tensor")
+    tt = []
+    for _ in range(max(5, args.steps // 2)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        tt.append(net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_fw.data_ptr(), graph=True,
+                                    contraction="tensor"))
+    ms_t = rep.max(float(np.mean(tt)))
+    contraction = {"popc_ms_per_step": ms, "tensor_ms_per_step": ms_t, "tensor_value": world * events / (ms_t / 1e3),
+                   "tensor_bit_exact": tensor_exact, "kept": "popc" if ms <= ms_t else "tensor",
+                   "note": "tensor = mma.sync m16n8k256 b1 and.popc, 8 entries x 32 rows per chunk; popc = __popc on "
+                           "the CUDA cores (the default path, timed as value)"}
+
     # plain GPU path on the same 300 trajectories (one persistent launch per trajectory)
     plain = None
     hbm_peak, pk = peaks()
@@ -653,6 +671,7 @@ def main() -> None:
         "e2e": {"value": world * events / e2e_s, "unit": "synaptic events/s", "h2d_bytes_per_step": int(cues.nbytes),
                 "d2h_bytes_per_step": int(B * NCOL * 4)},
         "wave_variant": wave,
+        "contraction_ab": contraction,
         "plain": plain,
         "batched_over_plain": (value / plain["value"]) if plain else None,
         "plain_train": ptrain,

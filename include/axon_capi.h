@@ -173,8 +173,14 @@ typedef struct axon_recall_args {
   uint32_t graph;       /* batched method: 1 = run the launch(es) and their buffer resets as a
                            captured CUDA graph, kept and replayed while every argument and
                            array stays the same (device-resident callers); 0 = launch directly */
-  uint32_t reserved[3]; /* zero */
+  uint32_t contraction; /* batched method: the unit that computes k_drive's AND-popcounts
+                           (src/axon.mm:166-173): AXON_CONTRACT_POPC (0, __popc on the CUDA
+                           cores) or AXON_CONTRACT_TENSOR (1, binary MMA on the tensor cores);
+                           the results are the same */
+  uint32_t reserved[2]; /* zero */
 } axon_recall_args;
+
+enum { AXON_CONTRACT_POPC = 0, AXON_CONTRACT_TENSOR = 1 };
 
 axon_status axon_recall(axon_net* net, const uint32_t* cues, uint32_t B, const axon_recall_args* args,
                         const uint32_t* ref_ball, uint32_t* final_spk, uint32_t* hist, uint32_t* stats,

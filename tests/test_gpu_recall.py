@@ -176,3 +176,28 @@ def test_final_spikes_into_caller_array():
         buf[:] = 0
     with pytest.raises(AssertionError):
         gpu.recall(cues, 12, 5, final_out=np.zeros((cues.shape[0], cfg.ncol), dtype=np.int32))
+
+
+@pytest.mark.parametrize("variant", [{}, dict(mode=0, dthr=2), dict(mode=2, dthr=0, boost=9), dict(ktest=5, facil=40),
+                                     dict(boost=2000)])
+def test_tensor_contraction_matches_oracle(variant):
+    """contraction="tensor" (binary MMA on the tensor cores) gives every trajectory the same
+    spikes at every step as the CUDA-core popcounts and as the oracle, packed 16-bit counters
+    and 32-bit ones (boost=2000) alike, with multi-word entries (clamped input groups)."""
+    cfg, gpu, cpu, pats = trained_pair(variant, 6, 2, 16)
+    cues = make_cues(pats, cfg.ncol, 37, np.random.default_rng(5))
+    rt = gpu.recall(cues, 20, 5, hist=True, stats=True, contraction="tensor")
+    rp = gpu.recall(cues, 20, 5, hist=True, stats=True)
+    assert np.array_equal(rt["hist"], rp["hist"]) and np.array_equal(rt["stats"], rp["stats"])
+    f, h, _, _ = oracle_runs(cpu, cues[:5], 20, 5, 0)
+    assert np.array_equal(rt["hist"][:5], h) and np.array_equal(rt["final"][:5], f)
+
+
+def test_tensor_contraction_full_geometry():
+    """Config C at full size, 300 cues of 45 steps: the tensor contraction equals the
+    CUDA-core one on every trajectory and step (several trajectories per CTA included)."""
+    cfg, gpu, cpu, pats = trained_pair(dict(ncol=4096, incols=512, target=64, k=24), 12, 2, 64)
+    cues = make_cues(pats, cfg.ncol, 300, np.random.default_rng(2))
+    rt = gpu.recall(cues, 45, 10, hist=True, contraction="tensor")
+    rp = gpu.recall(cues, 45, 10, hist=True)
+    assert np.array_equal(rt["hist"], rp["hist"])
