@@ -113,30 +113,28 @@ __device__ __forceinline__ void mma_units(const uint32_t* cPC, const uint32_t* c
     mma_b1_and(c1, a2, b0, b1);
     // the trajectories of entries 2q and 2q+1 (held by lanes 8q and 8q + 4)
     const uint32_t bA = __shfl_sync(kFull, bq, 8u * q), bB = __shfl_sync(kFull, bq, 8u * q + 4u);
-    // terms by row block k (rows g4 + 8k): tA for entry 2q, tB for entry 2q+1
-    uint32_t tA[4], tB[4];
-    tA[0] = branch_term<LIN>(c0[0], dthr, bst); tB[0] = branch_term<LIN>(c0[1], dthr, bst);
-    tA[1] = branch_term<LIN>(c0[2], dthr, bst); tB[1] = branch_term<LIN>(c0[3], dthr, bst);
-    tA[2] = branch_term<LIN>(c1[0], dthr, bst); tB[2] = branch_term<LIN>(c1[1], dthr, bst);
-    tA[3] = branch_term<LIN>(c1[2], dthr, bst); tB[3] = branch_term<LIN>(c1[3], dthr, bst);
+    // counts by row block k (rows g4 + 8k): cA for entry 2q, cB for entry 2q+1
+    const uint32_t cA[4] = {c0[0], c0[2], c1[0], c1[2]}, cB[4] = {c0[1], c0[3], c1[1], c1[3]};
     uint32_t* rowA = bA != kNone ? accB + ((sp >> 5) * B + bA) * accStride : nullptr;
     uint32_t* rowB = bB != kNone ? accB + ((sp >> 5) * B + bB) * accStride : nullptr;
     if (PACK) {
       // rows g4 and g4 ^ 1 share a counter word: the even lane adds entry 2q's pair, the odd
-      // lane entry 2q+1's
+      // lane entry 2q+1's; both terms of a word at once (see acc_add4c)
       const bool ev = (g4 & 1u) == 0u;
+      const uint32_t kk = (0x8000u - min(dthr, 0x8000u)) * 0x00010001u;
+      uint32_t* row = ev ? rowA : rowB;
 #pragma unroll
       for (uint32_t k = 0; k < 4; ++k) {
-        const uint32_t x = __shfl_xor_sync(kFull, ev ? tB[k] : tA[k], 4);
-        const uint32_t pr = ((g4 & ~1u) + 8u * k) >> 1;
-        if (ev) { if (rowA) atomicAdd(rowA + pr, tA[k] | (x << 16)); }
-        else if (rowB) atomicAdd(rowB + pr, x | (tB[k] << 16));
+        const uint32_t x = __shfl_xor_sync(kFull, ev ? cB[k] : cA[k], 4);
+        const uint32_t P = ev ? (cA[k] | (x << 16)) : (x | (cB[k] << 16));
+        const uint32_t N = ((P + kk) >> 15) & 0x00010001u;
+        if (row) atomicAdd(row + (((g4 & ~1u) + 8u * k) >> 1), LIN ? P + bst * N : N);
       }
     } else {
 #pragma unroll
       for (uint32_t k = 0; k < 4; ++k) {
-        if (rowA) atomicAdd(rowA + g4 + 8u * k, tA[k]);
-        if (rowB) atomicAdd(rowB + g4 + 8u * k, tB[k]);
+        if (rowA) atomicAdd(rowA + g4 + 8u * k, branch_term<LIN>(cA[k], dthr, bst));
+        if (rowB) atomicAdd(rowB + g4 + 8u * k, branch_term<LIN>(cB[k], dthr, bst));
       }
     }
   }
@@ -325,9 +323,8 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
 #pragma unroll
           for (uint32_t r = 0; r < 32u; r += 4) {
             const uint4 a = *reinterpret_cast<const uint4*>(tile + w3r_pos(r, w));
-            acc_add4<PACK>(accb, r, branch_term<LIN>(__popc(a.x & S), dthr, bst),
-                           branch_term<LIN>(__popc(a.y & S), dthr, bst), branch_term<LIN>(__popc(a.z & S), dthr, bst),
-                           branch_term<LIN>(__popc(a.w & S), dthr, bst));
+            acc_add4c<PACK, LIN>(accb, r, __popc(a.x & S), __popc(a.y & S), __popc(a.z & S), __popc(a.w & S), dthr,
+                                 bst);
           }
         } else {  // several nonzero words: counts in registers (words past the third from the spikes)
           const uint4 en = __ldcg(eMIn + (size_t)g * B + e);
@@ -351,8 +348,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
           }
 #pragma unroll
           for (int r = 0; r < 32; r += 4)
-            acc_add4<PACK>(accb, r, branch_term<LIN>(cnt[r], dthr, bst), branch_term<LIN>(cnt[r + 1], dthr, bst),
-                           branch_term<LIN>(cnt[r + 2], dthr, bst), branch_term<LIN>(cnt[r + 3], dthr, bst));
+            acc_add4c<PACK, LIN>(accb, r, cnt[r], cnt[r + 1], cnt[r + 2], cnt[r + 3], dthr, bst);
         }
       }
       if (__syncthreads_or(!ok)) {

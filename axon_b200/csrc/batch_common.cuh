@@ -60,19 +60,27 @@ constexpr uint32_t kColWords = kNslot * 256;             // one column's 32 tile
 constexpr uint64_t kDrainNs = 1000000000ull;             // bound on waiting for own copies after a timeout
 constexpr uint32_t kItemWords = kRecallCpi * kColWords;  // one work item
 
-template <bool PACK>
-__device__ __forceinline__ void acc_add4(uint32_t* accb, uint32_t r, uint32_t t0, uint32_t t1, uint32_t t2,
-                                         uint32_t t3) {
+// The dendritic terms of four counts (rows r..r+3) added into the counters. Packed counters
+// compute two terms at once in one word: with the counts c0, c1 (each below 2^15) in the
+// low and high halves, adding 0x8000 - dthr to each half sets bit 15 of a half exactly when
+// its count reaches dthr (no half carries into the next), so the terms are
+// P + bst * N (modes 0, 1) or N (mode 2), N the two threshold bits moved to bit 0 of their
+// halves. The host keeps packing for drives below 2^16, so no half overflows.
+template <bool PACK, bool LIN>
+__device__ __forceinline__ void acc_add4c(uint32_t* accb, uint32_t r, uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                          uint32_t dthr, uint32_t bst) {
   if (PACK) {
-    atomicAdd(accb + (r >> 1), t0 | (t1 << 16));
-    atomicAdd(accb + (r >> 1) + 1, t2 | (t3 << 16));
+    const uint32_t k = (0x8000u - min(dthr, 0x8000u)) * 0x00010001u;
+    const uint32_t p0 = c0 | (c1 << 16), p1 = c2 | (c3 << 16);
+    const uint32_t n0 = ((p0 + k) >> 15) & 0x00010001u, n1 = ((p1 + k) >> 15) & 0x00010001u;
+    atomicAdd(accb + (r >> 1), LIN ? p0 + bst * n0 : n0);
+    atomicAdd(accb + (r >> 1) + 1, LIN ? p1 + bst * n1 : n1);
   } else {
-    atomicAdd(accb + r, t0);
-    atomicAdd(accb + r + 1, t1);
-    atomicAdd(accb + r + 2, t2);
-    atomicAdd(accb + r + 3, t3);
+    atomicAdd(accb + r, branch_term<LIN>(c0, dthr, bst));
+    atomicAdd(accb + r + 1, branch_term<LIN>(c1, dthr, bst));
+    atomicAdd(accb + r + 2, branch_term<LIN>(c2, dthr, bst));
+    atomicAdd(accb + r + 3, branch_term<LIN>(c3, dthr, bst));
   }
 }
-
 
 }  // namespace axon

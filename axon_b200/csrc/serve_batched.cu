@@ -187,9 +187,8 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
 #pragma unroll
         for (uint32_t r = 0; r < 32u; r += 4) {
           const uint4 a = *reinterpret_cast<const uint4*>(tile + w3r_pos(r, w));
-          acc_add4<PACK>(accb, r, branch_term<LIN>(__popc(a.x & S), dthr, bst),
-                         branch_term<LIN>(__popc(a.y & S), dthr, bst), branch_term<LIN>(__popc(a.z & S), dthr, bst),
-                         branch_term<LIN>(__popc(a.w & S), dthr, bst));
+          acc_add4c<PACK, LIN>(accb, r, __popc(a.x & S), __popc(a.y & S), __popc(a.z & S), __popc(a.w & S), dthr,
+                               bst);
         }
       } else {  // several nonzero words: counts in registers (words past the third from the spikes)
         const uint4 en = __ldcg(eMIn + (size_t)g * kServeMaxB + e);
@@ -213,8 +212,7 @@ __global__ void __launch_bounds__(896, 1) k_serve_batched(ServeDev d, ServeCfg c
         }
 #pragma unroll
         for (int r = 0; r < 32; r += 4)
-          acc_add4<PACK>(accb, r, branch_term<LIN>(cnt[r], dthr, bst), branch_term<LIN>(cnt[r + 1], dthr, bst),
-                         branch_term<LIN>(cnt[r + 2], dthr, bst), branch_term<LIN>(cnt[r + 3], dthr, bst));
+          acc_add4c<PACK, LIN>(accb, r, cnt[r], cnt[r + 1], cnt[r + 2], cnt[r + 3], dthr, bst);
       }
     }
     if (__syncthreads_or(!ok)) {

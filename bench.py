@@ -489,14 +489,15 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def time_device(net, d_cues, B, T, clamp, d_final, flush, steps) -> list[float]:
+def time_device(net, d_cues, B, T, clamp, d_final, flush, steps, contraction="popc") -> list[float]:
     import torch
 
     times = []
     for _ in range(steps):
         flush.zero_()  # evict L2 between timed steps (untimed: outside the device-timed launch)
         torch.cuda.synchronize()
-        times.append(net.recall_device(d_cues.data_ptr(), B, T, clamp, d_final.data_ptr(), graph=True))
+        times.append(net.recall_device(d_cues.data_ptr(), B, T, clamp, d_final.data_ptr(), graph=True,
+                                       contraction=contraction))
     torch.cuda.synchronize()
     return times
 
@@ -509,6 +510,9 @@ def main() -> None:
     ap.add_argument("--impl", default="axon", choices=["axon", "reference"])
     ap.add_argument("--ref-traj", type=int, default=30)
     ap.add_argument("--cpu-traj", type=int, default=120)
+    ap.add_argument("--contraction", default="popc", choices=["popc", "tensor"],
+                    help="AND-popcount unit of the timed batched recall (the other one is timed in the A/B block)")
+    ap.add_argument("--no-ab", action="store_true", help="skip the contraction A/B and the wave variant")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffer) measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
@@ -550,7 +554,8 @@ def main() -> None:
     B = cues.shape[0]
     # events of the workload (fixed by the trajectories), from one recorded run, and every
     # trajectory against the oracle's fixture
-    ref = net.recall(cues, T_RECALL, CLAMP_RECALL, hist=True)
+    ctr = args.contraction
+    ref = net.recall(cues, T_RECALL, CLAMP_RECALL, hist=True, contraction=ctr)
     conn = net.read("CONN")
     ev = events_per_step(ref["hist"], conn)
     events = float(ev.sum())
@@ -562,12 +567,12 @@ def main() -> None:
     d_final = torch.empty((B, NCOL), dtype=torch.int32, device=f"cuda:{dev}")
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=f"cuda:{dev}")
     for _ in range(args.warmup):  # the first call captures the launch as a CUDA graph, the rest replay it
-        net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_final.data_ptr(), graph=True)
+        net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_final.data_ptr(), graph=True, contraction=ctr)
     assert np.array_equal(d_final.cpu().numpy().view(np.uint32), ref["final"])
     torch.cuda.synchronize()
     rep.barrier()
     with ClockSampler(dev) as clk:
-        times = time_device(net, d_cues, B, T_RECALL, CLAMP_RECALL, d_final, flush, args.steps)
+        times = time_device(net, d_cues, B, T_RECALL, CLAMP_RECALL, d_final, flush, args.steps, ctr)
     rep.barrier()
     ms = rep.max(float(np.mean(times)))
     value = world * events / (ms / 1e3)
@@ -579,7 +584,7 @@ def main() -> None:
     for it in range(0 if args.no_e2e else args.warmup + max(3, args.steps // 2)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r = net.recall(h_cues, T_RECALL, CLAMP_RECALL, graph=True, final_out=h_final)
+        r = net.recall(h_cues, T_RECALL, CLAMP_RECALL, graph=True, final_out=h_final, contraction=ctr)
         dt = time.perf_counter() - t0
         if it >= args.warmup:
             e2e_t.append(dt)
@@ -587,36 +592,37 @@ def main() -> None:
         assert np.array_equal(r["final"], ref["final"])
     e2e_s = rep.max(float(np.mean(e2e_t)) if e2e_t else float("nan"))
 
-    # the reference-parity variant: the wave readout's 5 clamped + 30 free steps
-    rw = net.recall(cues, T_WAVE, CLAMP_WAVE, hist=True)
-    ev_w = float(events_per_step(rw["hist"], conn).sum())
-    d_fw = torch.empty((B, NCOL), dtype=torch.int32, device=f"cuda:{dev}")
-    for _ in range(args.warmup):
-        net.recall_device(d_cues.data_ptr(), B, T_WAVE, CLAMP_WAVE, d_fw.data_ptr(), graph=True)
-    assert np.array_equal(d_fw.cpu().numpy().view(np.uint32), rw["final"])
-    tw = time_device(net, d_cues, B, T_WAVE, CLAMP_WAVE, d_fw, flush, max(5, args.steps // 2))
-    ms_w = rep.max(float(np.mean(tw)))
-    wave = {"workload": "the same 300 cues x (5 clamp + 30 free), the reference's wave readout (src/axon.mm:1804-1858)",
-            "value": world * ev_w / (ms_w / 1e3), "unit": "synaptic events/s", "ms_per_step": ms_w,
-            "events_per_batch": ev_w}
-
-    # A/B of the contraction unit: the same batch with k_drive's AND-popcounts on the tensor
-    # cores (binary MMA, m16n8k256 and.popc) instead of __popc on the CUDA cores
-    rt = net.recall(cues, T_RECALL, CLAMP_RECALL, hist=True, contraction="tensor")
-    tensor_exact = bool(np.array_equal(rt["hist"], ref["hist"]))
-    for _ in range(args.warmup):
-        net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_fw.data_ptr(), graph=True, contraction="tensor")
-    tt = []
-    for _ in range(max(5, args.steps // 2)):
-        flush.zero_()
-        torch.cuda.synchronize()
-        tt.append(net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_fw.data_ptr(), graph=True,
-                                    contraction="tensor"))
-    ms_t = rep.max(float(np.mean(tt)))
-    contraction = {"popc_ms_per_step": ms, "tensor_ms_per_step": ms_t, "tensor_value": world * events / (ms_t / 1e3),
-                   "tensor_bit_exact": tensor_exact, "kept": "popc" if ms <= ms_t else "tensor",
-                   "note": "tensor = mma.sync m16n8k256 b1 and.popc, 8 entries x 32 rows per chunk; popc = __popc on "
-                           "the CUDA cores (the default path, timed as value)"}
+    wave = contraction = None
+    if not args.no_ab:
+        # the reference-parity variant: the wave readout's 5 clamped + 30 free steps
+        rw = net.recall(cues, T_WAVE, CLAMP_WAVE, hist=True, contraction=ctr)
+        ev_w = float(events_per_step(rw["hist"], conn).sum())
+        d_fw = torch.empty((B, NCOL), dtype=torch.int32, device=f"cuda:{dev}")
+        for _ in range(args.warmup):
+            net.recall_device(d_cues.data_ptr(), B, T_WAVE, CLAMP_WAVE, d_fw.data_ptr(), graph=True, contraction=ctr)
+        assert np.array_equal(d_fw.cpu().numpy().view(np.uint32), rw["final"])
+        tw = time_device(net, d_cues, B, T_WAVE, CLAMP_WAVE, d_fw, flush, max(5, args.steps // 2), ctr)
+        ms_w = rep.max(float(np.mean(tw)))
+        wave = {"workload": "the same 300 cues x (5 clamp + 30 free), the reference's wave readout "
+                            "(src/axon.mm:1804-1858)",
+                "value": world * ev_w / (ms_w / 1e3), "unit": "synaptic events/s", "ms_per_step": ms_w,
+                "events_per_batch": ev_w}
+        # A/B of the contraction unit: the same batch with k_drive's AND-popcounts on the other
+        # unit (tensor cores: binary MMA m16n8k256 and.popc; CUDA cores: __popc)
+        other = "tensor" if ctr == "popc" else "popc"
+        ro = net.recall(cues, T_RECALL, CLAMP_RECALL, hist=True, contraction=other)
+        other_exact = bool(np.array_equal(ro["hist"], ref["hist"]))
+        for _ in range(args.warmup):
+            net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_fw.data_ptr(), graph=True,
+                              contraction=other)
+        to = time_device(net, d_cues, B, T_RECALL, CLAMP_RECALL, d_fw, flush, max(5, args.steps // 2), other)
+        ms_o = rep.max(float(np.mean(to)))
+        per = {ctr: ms, other: ms_o}
+        contraction = {"popc_ms_per_step": per["popc"], "tensor_ms_per_step": per["tensor"],
+                       "timed_as_value": ctr, f"{other}_bit_exact": other_exact,
+                       "faster": min(per, key=per.get),
+                       "note": "tensor = mma.sync m16n8k256 b1 and.popc, 8 entries x 32 rows per chunk; popc = __popc "
+                               "on the CUDA cores"}
 
     # plain GPU path on the same 300 trajectories (one persistent launch per trajectory)
     plain = None
