@@ -8,6 +8,7 @@ namespace axon {
 
 constexpr uint32_t kRecallMaxB = 512;   // trajectories per launch (the host splits larger batches)
 constexpr uint32_t kRecallCpi = 2;      // columns per phase-1 work item
+constexpr uint32_t kRecallMaxT = 1024;  // steps of a batched readout without per-step records
 
 // Device buffers of one batched recall launch over B trajectories of one network.
 struct RecallDev {
@@ -29,7 +30,7 @@ struct RecallDev {
   uint32_t* driveLog;       // [B][256] member-drive log (accumulated), or null
   uint32_t* theta;          // [B] threshold of the last step, or null
   uint32_t* thPrev;         // [B] each trajectory's latest threshold (zeroed before launch)
-  uint32_t* work;           // [T] phase-1 work counters (zeroed before launch)
+  uint32_t* work;           // [max(T, 64)] phase-1 work counters (zeroed before launch)
   uint32_t* bar;            // grid barrier counter (zeroed before launch)
   uint32_t* err;            // device error word
 };

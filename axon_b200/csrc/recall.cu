@@ -56,7 +56,12 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
                              double* ms) {
   if (!initialized) return set_error(AXON_ESTATE, "recall before init");
   if (B == 0) return set_error(AXON_EINVAL, "B must be >= 1");
-  if (a.T == 0 || a.T > 64) return set_error(AXON_EINVAL, "T must be in 1..64");
+  // the per-step records (hist, stats, driveLog) and the plain path's network buffers hold
+  // 64 steps, as the reference's do; a batched readout that keeps none of them runs longer
+  const bool records = hist || stats || driveLog || refBall || a.method == AXON_RECALL_PLAIN;
+  if (a.T == 0 || a.T > (records ? 64u : kRecallMaxT))
+    return set_error(AXON_EINVAL, records ? "T must be in 1..64 (per-step records or the plain method)"
+                                          : "T must be in 1..1024");
   if (a.use_bias > 1 || a.method > 1 || a.contraction > 1)
     return set_error(AXON_EINVAL, "bad use_bias, method or contraction");
   CK(cudaSetDevice(device));
@@ -136,7 +141,7 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     const size_t bnc = (size_t)Bc * ncol;
     const size_t accBytes = bnc * 32 * (rc.acc32 ? 4 : 2);
     const size_t need = al(2 * bnc * 4) + al(2ull * ngrp * Bc * 8) + al(2ull * ngrp * Bc * 16) + al(4ull * ngrp * 4) + al(bnc * 4) +
-                        al(accBytes) + al(64 * 4) + al((size_t)Bc * 4);
+                        al(accBytes) + al((size_t)std::max(a.T, 64u) * 4) + al((size_t)Bc * 4);
     st = scratch.ensure(need);
     if (st != AXON_OK) return st;
     char* p = (char*)scratch.p;
@@ -152,7 +157,7 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     rd.ecnt = (uint32_t*)take(4ull * ngrp * 4);
     rd.drv = (uint32_t*)take(bnc * 4);
     rd.acc = take(accBytes);
-    rd.work = (uint32_t*)take(64 * 4);
+    rd.work = (uint32_t*)take((size_t)std::max(a.T, 64u) * 4);
     rd.thPrev = (uint32_t*)take((size_t)Bc * 4);
     rd.theta = nullptr;
     rd.bar = d.bar;
@@ -190,7 +195,7 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
       rd.driveLog = dLog ? dLog + (size_t)b0 * 256 : nullptr;
       if (e == cudaSuccess) e = cudaMemsetAsync(rd.spk, 0, (size_t)nb * ncol * 4, stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(rd.ecnt, 0, 2ull * ngrp * 4, stream);
-      if (e == cudaSuccess) e = cudaMemsetAsync(rd.work, 0, 64 * 4, stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(rd.work, 0, (size_t)std::max(a.T, 64u) * 4, stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(rd.thPrev, 0, (size_t)nb * 4, stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(d.bar, 0, 4, stream);
       if (e == cudaSuccess) e = launch_recall(rd, rc, rs, stream);

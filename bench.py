@@ -276,19 +276,23 @@ def bench_serve(dev: int, rates=SERVE_RATES, seconds: float = SERVE_SECONDS, nne
                 st = srv.stats()
             finally:
                 srv.close()
-            # after the timed window: each checked request alone through the plain path
+            # after the timed window: each checked request alone through the plain path (64
+            # steps at most, the length its per-step records hold), longer ones through a
+            # batched recall of that one trajectory
             ncheck = n if SERVE_CHECK.get(rate) is None else min(n, SERVE_CHECK[rate])
             checked = reqs[:: max(1, n // ncheck)][:ncheck]
-            mism = 0
+            mism = nplain = 0
             for tg, net, q, cols, free in checked:
-                alone = nets[net].recall(ax.clamp_words(cols, NCOL)[None, :], 5 + free, 5, method="plain")["final"][0]
+                method = "plain" if 5 + free <= 64 else "batched"
+                nplain += method == "plain"
+                alone = nets[net].recall(ax.clamp_words(cols, NCOL)[None, :], 5 + free, 5, method=method)["final"][0]
                 mism += int(not np.array_equal(alone, results[tg]))
             lat_ms = np.array(lat) * 1e3
             out["rates"].append({"offered_req_s": rate, "requests": n,
                                  "trajectories_per_s": n / (last - float(arrive[0])),
                                  "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
                                  "mean_overlap_with_reference": float(np.mean(ov)),
-                                 "checked": len(checked), "mismatches": mism,
+                                 "checked": len(checked), "checked_plain": nplain, "mismatches": mism,
                                  "mean_batch": st["mean_batch"], "max_batch": st["max_batch"]})
             tag += n
     finally:

@@ -166,7 +166,8 @@ uint32_t axon_noisy_cue_seed(uint32_t q, uint32_t pct, uint32_t draw);
 typedef enum axon_recall_method { AXON_RECALL_BATCHED = 0, AXON_RECALL_PLAIN = 1 } axon_recall_method;
 
 typedef struct axon_recall_args {
-  uint32_t T;           /* steps per trajectory, 1..64 */
+  uint32_t T;           /* steps per trajectory, 1..64; up to 1024 for the batched method when
+                           hist, stats, drive_log and ref_ball are all NULL */
   uint32_t clamp_steps; /* leading steps clamped to the cue */
   uint32_t use_bias;    /* 0 off (the reference's readout default), 1 on */
   uint32_t method;      /* axon_recall_method */

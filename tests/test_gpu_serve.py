@@ -126,3 +126,27 @@ def test_variants_in_the_mix_equal_recall(variant):
     finally:
         for n in nets:
             n.close()
+
+
+def test_long_requests_equal_long_batched_recall(fleet):
+    """Requests longer than the 64 steps the per-step records hold (the server keeps none):
+    their final spikes equal a batched axon_recall of the same length run alone and in a
+    batch (the batched method takes up to 1024 steps when it keeps no per-step records),
+    and the first 64 steps equal the plain method's."""
+    nets, pats = fleet
+    reqs = [dict(tag=i, net=i % 3, cols=np.sort(pats[i % 3][i % LOADS[i % 3]][: 4 + i]).astype(np.uint32), free=f)
+            for i, f in enumerate([59, 60, 75, 123])]
+    got, _ = serve(nets, reqs)
+    for r in reqs:
+        net = nets[r["net"]]
+        cue = ax.clamp_words(r["cols"], net.ncol)[None, :]
+        alone = net.recall(cue, CLAMP + r["free"], CLAMP)["final"][0]
+        assert np.array_equal(got[r["tag"]][1], alone), r["tag"]
+        batch = net.recall(np.repeat(cue, 5, axis=0), CLAMP + r["free"], CLAMP)["final"]
+        assert all(np.array_equal(b, alone) for b in batch)
+    r = reqs[0]  # 64 steps: also the plain method
+    assert np.array_equal(got[r["tag"]][1], alone_by_recall(nets, r))
+    from axon_b200._capi import AxonError
+
+    with pytest.raises(AxonError):
+        nets[0].recall(ax.clamp_words(reqs[2]["cols"], nets[0].ncol)[None, :], 80, CLAMP, hist=True)
