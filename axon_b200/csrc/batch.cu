@@ -304,15 +304,21 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         if (lane == 0) u = atomicAdd(sMisc + 6 + bcur, 1u);
         u = __shfl_sync(kFull, u, 0);
         if (u >= units) break;
-        uint32_t flat = u * 32u + lane;
+        // the branch of each list (multi-word, single-word) that holds the unit's first entry
+        // of that list: the number of branches ending at or before it; a lane then steps over
+        // the few branch boundaries between that entry and its own
+        const uint32_t f0 = u * 32u, fM = min(f0, EM), f1 = f0 > EM ? f0 - EM : 0u;
+        const uint32_t spM = (uint32_t)__popc(__ballot_sync(kFull, cPM[lane + 1] <= fM)) +
+                             (uint32_t)__popc(__ballot_sync(kFull, cPM[lane + 33] <= fM));
+        const uint32_t sp1 = (uint32_t)__popc(__ballot_sync(kFull, cP1[lane + 1] <= f1)) +
+                             (uint32_t)__popc(__ballot_sync(kFull, cP1[lane + 33] <= f1));
+        uint32_t flat = f0 + lane;
         if (flat >= E) continue;
         const bool single = flat >= EM;
         const uint32_t* P = single ? cP1 : cPM;
         if (single) flat -= EM;
-        uint32_t sp = 0;
-#pragma unroll
-        for (uint32_t step = 32; step; step >>= 1)
-          if (sp + step < 64u && P[sp + step] <= flat) sp += step;
+        uint32_t sp = single ? sp1 : spM;
+        while (P[sp + 1] <= flat) ++sp;
         const uint32_t e = flat - P[sp];
         const uint32_t g = cConn[sp];
         const uint32_t* tile = tileBase + (sp >> 5) * kColWords + (sp & 31u) * 256u;
