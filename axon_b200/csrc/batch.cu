@@ -17,13 +17,17 @@
 //            cost nothing. The counters then become the per-neuron and column drives, and
 //            the write-back that reads them clears them. One CTA barrier per item separates
 //            its units from its write-back; with two counter buffers nothing else does.
-//   phase 2  per trajectory: the column threshold (block_theta), the exact k-of-32 ballot
-//            only for columns that pass the gate, the new spike vector, and its group lists.
+//            The write-back also counts every recurrent column drive into the trajectory's
+//            drive histogram for the step (count, largest and smallest drive per bin).
+//   phase 2  per trajectory: the column threshold from that histogram (hist_theta), the
+//            exact k-of-32 ballot only for columns that pass the gate, the new spike
+//            vector, and its group lists.
 #include <cstdint>
 
 #include "axon_device.cuh"
 #include "batch.cuh"
 #include "batch_common.cuh"
+#include "plain.cuh"
 #include "theta.cuh"
 
 namespace axon {
@@ -140,6 +144,35 @@ __device__ __forceinline__ void mma_units(const uint32_t* cPC, const uint32_t* c
   }
 }
 
+// The smallest drive a trajectory's histogram records in a step: the lower edge of the bin
+// of half the threshold of its previous step (at least 1), so every bin is recorded whole or
+// not at all. The threshold is the target-th largest recurrent drive, so when at least
+// `target` drives reach the floor the histogram holds every drive that can be the answer,
+// and each of their bins completely; otherwise phase 2 falls back to sorting all drives.
+// Counting only these columns keeps the write-back's atomics few and off the crowded low
+// bins.
+__device__ __forceinline__ uint32_t hist_floor(const uint32_t* thPrev) {
+  return theta_bin_lo(theta_key(min(max(__ldcg(thPrev) >> 1, 1u), (1u << 24) - 1u)));
+}
+
+// One recurrent column drive into a threshold histogram (theta_key bins: count, largest
+// drive, complement of the smallest), as the plain path's phase A counts them.
+__device__ __forceinline__ void count_drive(uint32_t* h, uint32_t drv) {
+  if (drv >= (1u << 24)) return;  // never a threshold candidate (src/axon.mm:276)
+  h += theta_key(drv);
+  atomicAdd(h, 1u);
+  atomicMax(h + kThetaBins, drv);
+  atomicMax(h + 2u * kThetaBins, ~drv);
+}
+
+// The threshold select of phase 2, kept out of line so that its registers do not add to
+// phase 1's.
+static __device__ __noinline__ uint32_t recall_theta(const uint32_t* sD, const uint32_t* sH, uint32_t* sCand,
+                                                     uint32_t* sCtl, uint32_t incols, uint32_t ncol, uint32_t need,
+                                                     uint32_t topkPar) {
+  return hist_theta<-1>(sD, sH, sCand, sCtl, incols, ncol, need, topkPar);
+}
+
 // MMA: the AND-popcount contraction of phase 1 on the tensor cores (mma.sync b1 and.popc,
 // m16n8k256: 16 tile rows x 8 entries x the group's 256 spike bits per instruction) instead
 // of __popc on the CUDA cores; the dendritic terms, counters and everything else are shared.
@@ -161,8 +194,12 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   // phase-2 views reuse the tile buffers; a second drive buffer follows them when it fits
   uint32_t* sSpk = sTile + ncol;
   uint32_t* sList = sTile + 2 * ncol;
-  uint32_t* sRed = sTile + 3 * ncol;  // 192 words
-  uint32_t* sHist = sRed + 192;
+  uint32_t* sRed = sTile + 3 * ncol;  // 192 words and
+  uint32_t* sHist = sRed + 192;       // 256 words of the sorting threshold select
+  uint32_t* sCtl = sHist + 256;       // 64 words: histogram threshold-select control
+  // the trajectory's drive histogram (and, with two buffers, the next one's drives and
+  // histogram) follow
+  uint32_t* sH0 = sCtl + 64;
 
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
   const uint32_t nitems = (ncol + kRecallCpi - 1) / kRecallCpi;
@@ -374,20 +411,32 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       if (PACK && !c.useBias && !c.facil && d.refBall == nullptr) {
         // the packed counters already are the u16 drive slab: four lanes per (column,
         // trajectory), each storing 4 of its 16 words as one 16-byte vector
+        // (column, trajectory) pairs in column-major order: the trajectory index steps by
+        // 8 x warps, with no division
         const uint32_t q = lane & 3u, grp = lane >> 2;
         const uint32_t gmask = 0xFu << (grp * 4u);
-        for (uint32_t pp = warp * 8u + grp; pp < kRecallCpi * B; pp += nw * 8u) {
-          const uint32_t colL = pp / B, b = pp - colL * B, col = c0 + colL;
-          if (col >= ncol) continue;  // uniform over the four lanes
+        const uint32_t ncl = min(kRecallCpi, ncol - c0);
+        uint32_t colL = 0, b = warp * 8u + grp;
+        while (b >= B && colL < ncl) { b -= B; ++colL; }
+        while (colL < ncl) {  // uniform over the four lanes of a pair
+          const uint32_t col = c0 + colL;
           uint32_t* src = accB + (colL * B + b) * accStride + q * 4u;
           const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
           src[0] = src[1] = src[2] = src[3] = 0u;
-          reinterpret_cast<uint4*>(d.acc)[(((size_t)b * ncol + col) * 16u >> 2) + q] = w;
-          uint32_t s = (w.x & 0xFFFFu) + (w.x >> 16) + (w.y & 0xFFFFu) + (w.y >> 16) + (w.z & 0xFFFFu) + (w.z >> 16) +
-                       (w.w & 0xFFFFu) + (w.w >> 16);
+          reinterpret_cast<uint4*>(d.acc)[((size_t)b * ncol + col) * 4u + q] = w;
+          // sum of the 8 per-neuron drives in w: each word is lo + 65536 hi, so lo + hi is
+          // the word minus 65535 hi
+          uint32_t s = (w.x - 65535u * (w.x >> 16)) + (w.y - 65535u * (w.y >> 16)) + (w.z - 65535u * (w.z >> 16)) +
+                       (w.w - 65535u * (w.w >> 16));
           s += __shfl_xor_sync(gmask, s, 1);
           s += __shfl_xor_sync(gmask, s, 2);
-          if (q == 0) __stcg(d.drv + (size_t)b * ncol + col, s);
+          if (q == 0) {
+            __stcg(d.drv + (size_t)b * ncol + col, s);
+            if (col >= incols && s >= hist_floor(d.thPrev + b))
+              count_drive(d.thHist + ((size_t)(t % 3u) * B + b) * kHistWords, s);
+          }
+          b += nw * 8u;
+          while (b >= B && colL < ncl) { b -= B; ++colL; }
         }
       } else {
         for (uint32_t pp = warp; pp < kRecallCpi * B; pp += nw) {
@@ -403,7 +452,11 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
           if (c.acc32) reinterpret_cast<uint32_t*>(d.acc)[((size_t)b * ncol + col) * 32u + lane] = a;
           else reinterpret_cast<uint16_t*>(d.acc)[((size_t)b * ncol + col) * 32u + lane] = (uint16_t)a;
           const uint32_t dsum = __reduce_add_sync(kFull, a);
-          if (lane == 0) __stcg(d.drv + (size_t)b * ncol + col, dsum);
+          if (lane == 0) {
+            __stcg(d.drv + (size_t)b * ncol + col, dsum);
+            if (col >= incols && dsum >= hist_floor(d.thPrev + b))
+              count_drive(d.thHist + ((size_t)(t % 3u) * B + b) * kHistWords, dsum);
+          }
           if (d.refBall != nullptr && col >= incols) {  // driveLog of k_emit, src/axon.mm:216-220
             const uint32_t rb = __ldg(d.refBall + (size_t)b * ncol + col);
             if (rb) {
@@ -426,29 +479,67 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     if (!grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;
 
     // ---------------- phase 2: threshold, gated k-of-32 ballots, next spike vectors and lists
-    // The column drives of the CTA's trajectories arrive by asynchronous copies; with two
-    // buffers the next trajectory's copy is in flight while the current one is processed.
-    const bool dbuf = 4u * ncol + 448u <= 2u * kItemWords;
-    uint32_t* const sDalt = sTile + 3u * ncol + 448u;
-    auto load_drv = [&](uint32_t b, uint32_t* dst) {
+    // The column drives and the drive histogram of the CTA's trajectories arrive by
+    // asynchronous copies; with two buffers the next trajectory's copies are in flight while
+    // the current one is processed.
+    const bool dbuf = 4u * ncol + 512u + 2u * kHistWords <= 2u * kItemWords;
+    uint32_t* const sD1 = sH0 + kHistWords;
+    uint32_t* const sH1 = sD1 + ncol;
+    const uint32_t* hStep = d.thHist + (size_t)(t % 3u) * B * kHistWords;
+    auto load_drv = [&](uint32_t b, uint32_t slot) {
       const uint4* src = reinterpret_cast<const uint4*>(d.drv + (size_t)b * ncol);
-      for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x) cp_async16(reinterpret_cast<uint4*>(dst) + i, src + i);
+      uint4* dst = reinterpret_cast<uint4*>(slot ? sD1 : sTile);
+      for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x) cp_async16(dst + i, src + i);
+      const uint4* hs = reinterpret_cast<const uint4*>(hStep + (size_t)b * kHistWords);
+      uint4* hd = reinterpret_cast<uint4*>(slot ? sH1 : sH0);
+      for (uint32_t i = tid; i < kHistWords / 4u; i += blockDim.x) cp_async16(hd + i, hs + i);
     };
-    if (blockIdx.x < B) load_drv(blockIdx.x, sTile);
+    // Tasks: trajectory blockIdx + k * grid for the full rounds k < F. The R < grid
+    // trajectories of the last round are split, when each can have at least two CTAs, into
+    // P = grid / R parts, each on a range of whole groups (8 columns): every part selects
+    // the same threshold, then gates, ballots, writes and lists only its own columns, so the
+    // last round costs about one threshold select instead of a whole trajectory.
+    const uint32_t G = gridDim.x, F = B / G, R = B - F * G;
+    const uint32_t P = R ? G / R : 0u;
+    const bool split = P >= 2u;
+    const uint32_t ntask = F + (R != 0u && blockIdx.x < (split ? R * P : R) ? 1u : 0u);
+    auto task_b = [&](uint32_t k) { return k < F ? blockIdx.x + k * G : F * G + (split ? blockIdx.x / P : blockIdx.x); };
+    if (ntask) load_drv(task_b(0), 0);
     cp_async_commit();
-    for (uint32_t b = blockIdx.x, k = 0; b < B; b += gridDim.x, ++k) {
-      uint32_t* sD = (dbuf && (k & 1u)) ? sDalt : sTile;
-      const uint32_t bNext = b + gridDim.x;
-      if (dbuf && bNext < B) load_drv(bNext, (k & 1u) ? sTile : sDalt);
+    for (uint32_t k = 0; k < ntask; ++k) {
+      const uint32_t b = task_b(k);
+      const bool part = split && k == F;
+      const uint32_t pi = part ? blockIdx.x % P : 0u, np = part ? P : 1u;
+      const uint32_t gLo = pi * ngrp / np, gHi = (pi + 1u) * ngrp / np, cLo = 8u * gLo, cHi = 8u * gHi;
+      const uint32_t slot = dbuf ? (k & 1u) : 0u;
+      uint32_t* sD = slot ? sD1 : sTile;
+      const uint32_t* sH = slot ? sH1 : sH0;
+      const bool hasNext = k + 1u < ntask;
+      if (dbuf && hasNext) load_drv(task_b(k + 1u), slot ^ 1u);
       cp_async_commit();
-      if (dbuf) cp_async_wait<1>();  // all but the copy just issued: this trajectory's drives
+      if (dbuf) cp_async_wait<1>();  // all but the copies just issued: this trajectory's
       else cp_async_wait<0>();
-      if (tid == 0) sMisc[4] = 0u;
+      if (tid == 0) { sMisc[4] = 0u; sCtl[0] = 0u; }
+      if (warp == 0) {  // drives the histogram holds
+        uint32_t n = 0;
+        for (uint32_t i = lane; i < kThetaBins; i += 32u) n += sH[i];
+        n = __reduce_add_sync(kFull, n);
+        if (lane == 0) sCtl[8] = n;
+      }
       __syncthreads();
-      const uint32_t theta = block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed, __ldcg(d.thPrev + b));
+      const uint32_t theta = sCtl[8] >= c.targetCols
+                                 ? recall_theta(sD, sH, sList, sCtl, incols, ncol, c.targetCols, c.topkPar)
+                                 : block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed,
+                                               __ldcg(d.thPrev + b));
+      // this trajectory's histogram of step t+1 mod 3, last read two steps ago, is cleared
+      // for phase 1 of the next step
+      if (pi == 0u) {
+        uint4* hz = reinterpret_cast<uint4*>(d.thHist + ((size_t)((t + 1u) % 3u) * B + b) * kHistWords);
+        for (uint32_t i = tid; i < kHistWords / 4u; i += blockDim.x) __stcg(hz + i, make_uint4(0u, 0u, 0u, 0u));
+      }
       const uint32_t gate = max(theta, 1u);
       const uint32_t* stimb = d.stims + (size_t)b * ncol;
-      for (uint32_t cc = tid; cc < ncol; cc += blockDim.x) {
+      for (uint32_t cc = cLo + tid; cc < cHi; cc += blockDim.x) {
         uint32_t v = 0u;
         if (clamp && cc < incols) v = __ldg(stimb + cc);
         else if (sD[cc] >= gate) sList[atomicAdd(sMisc + 4, 1u)] = cc;
@@ -496,14 +587,14 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       }
       __syncthreads();
       uint32_t* outb = spkOut + (size_t)b * ncol;
-      for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x) {
+      for (uint32_t i = cLo / 4u + tid; i < cHi / 4u; i += blockDim.x) {
         const uint4 v = reinterpret_cast<const uint4*>(sSpk)[i];
         __stcg(reinterpret_cast<uint4*>(outb) + i, v);
         if (d.hist) reinterpret_cast<uint4*>(d.hist + ((size_t)b * c.T + t) * ncol)[i] = v;
         if (d.finalOut && t + 1u == c.T) reinterpret_cast<uint4*>(d.finalOut + (size_t)b * ncol)[i] = v;
       }
       if (t + 1u < c.T) {  // group lists for the next step
-        for (uint32_t g = tid; g < ngrp; g += blockDim.x) {
+        for (uint32_t g = gLo + tid; g < gHi; g += blockDim.x) {
           const uint4 p = reinterpret_cast<const uint4*>(sSpk)[2 * g], q = reinterpret_cast<const uint4*>(sSpk)[2 * g + 1];
           const uint32_t w[8] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w};
           uint32_t nz = 0, S0 = 0u, S1 = 0u, S2 = 0u, k = 0, w0 = 0;
@@ -525,12 +616,12 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
           }
         }
       }
-      if (tid == 0) {
+      if (tid == 0 && pi == 0u) {
         __stcg(d.thPrev + b, theta);
         if (d.theta && t + 1u == c.T) d.theta[b] = theta;
       }
       __syncthreads();
-      if (!dbuf && bNext < B) load_drv(bNext, sTile);  // committed at the next trajectory's start
+      if (!dbuf && hasNext) load_drv(task_b(k + 1u), 0);  // committed at the next task's start
     }
     cp_async_wait<0>();
     if (t + 1u < c.T && !grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;

@@ -141,7 +141,7 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     const size_t bnc = (size_t)Bc * ncol;
     const size_t accBytes = bnc * 32 * (rc.acc32 ? 4 : 2);
     const size_t need = al(2 * bnc * 4) + al(2ull * ngrp * Bc * 8) + al(2ull * ngrp * Bc * 16) + al(4ull * ngrp * 4) + al(bnc * 4) +
-                        al(accBytes) + al((size_t)std::max(a.T, 64u) * 4) + al((size_t)Bc * 4);
+                        al(accBytes) + al((size_t)std::max(a.T, 64u) * 4) + al(3ull * Bc * kHistWords * 4) + al((size_t)Bc * 4);
     st = scratch.ensure(need);
     if (st != AXON_OK) return st;
     char* p = (char*)scratch.p;
@@ -158,6 +158,7 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     rd.drv = (uint32_t*)take(bnc * 4);
     rd.acc = take(accBytes);
     rd.work = (uint32_t*)take((size_t)std::max(a.T, 64u) * 4);
+    rd.thHist = (uint32_t*)take(3ull * Bc * kHistWords * 4);
     rd.thPrev = (uint32_t*)take((size_t)Bc * 4);
     rd.theta = nullptr;
     rd.bar = d.bar;
@@ -196,6 +197,7 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
       if (e == cudaSuccess) e = cudaMemsetAsync(rd.spk, 0, (size_t)nb * ncol * 4, stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(rd.ecnt, 0, 2ull * ngrp * 4, stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(rd.work, 0, (size_t)std::max(a.T, 64u) * 4, stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(rd.thHist, 0, 3ull * nb * kHistWords * 4, stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(rd.thPrev, 0, (size_t)nb * 4, stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(d.bar, 0, 4, stream);
       if (e == cudaSuccess) e = launch_recall(rd, rc, rs, stream);

@@ -118,6 +118,9 @@ __device__ __forceinline__ uint32_t theta_key(uint32_t d) {
   return ((e - 4u) << 5) | ((d >> (e - 5u)) & 31u);
 }
 
+// The smallest drive of theta_key bin k.
+__device__ __forceinline__ uint32_t theta_bin_lo(uint32_t k) { return k < 64u ? k : (32u | (k & 31u)) << ((k >> 5) - 1u); }
+
 // The same threshold as block_theta (src/axon.mm:301-352 and :259-292) when every
 // recurrent drive below 2^24 has been recorded in sH as it was published: per theta_key
 // bin the count (sH[0, 640)), the largest drive (sH[640, 1280)) and the complement of the
