@@ -191,6 +191,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   uint32_t* sPC = sPM + 2 * 68;                          // [2][68] MMA: chunks of 8 entries, prefix over branches
   uint32_t* sMisc = sPC + 2 * 68;  // [16]: grid barrier flag, first item, -, -, gated count, -, unit counters [2], next items [2]
   uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
+  uint32_t* sFloor = sMisc + 20;  // [B] each trajectory's histogram floor for this step
   // phase-2 views reuse the tile buffers; a second drive buffer follows them when it fits
   uint32_t* sSpk = sTile + ncol;
   uint32_t* sList = sTile + 2 * ncol;
@@ -278,6 +279,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     // next step's list lengths start at zero (last read in phase 1 of step t-1)
     if (blockIdx.x == 0)
       for (uint32_t g = tid; g < 2 * ngrp; g += blockDim.x) c1Out[g] = 0u;
+    for (uint32_t b = tid; b < B; b += blockDim.x) sFloor[b] = hist_floor(d.thPrev + b);  // read after the sync below
 
     // ---------------- phase 1
     // thread 0 claims one item ahead: the claim's round trip overlaps the current item
@@ -432,7 +434,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
           s += __shfl_xor_sync(gmask, s, 2);
           if (q == 0) {
             __stcg(d.drv + (size_t)b * ncol + col, s);
-            if (col >= incols && s >= hist_floor(d.thPrev + b))
+            if (col >= incols && s >= sFloor[b])
               count_drive(d.thHist + ((size_t)(t % 3u) * B + b) * kHistWords, s);
           }
           b += nw * 8u;
@@ -454,7 +456,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
           const uint32_t dsum = __reduce_add_sync(kFull, a);
           if (lane == 0) {
             __stcg(d.drv + (size_t)b * ncol + col, dsum);
-            if (col >= incols && dsum >= hist_floor(d.thPrev + b))
+            if (col >= incols && dsum >= sFloor[b])
               count_drive(d.thHist + ((size_t)(t % 3u) * B + b) * kHistWords, dsum);
           }
           if (d.refBall != nullptr && col >= incols) {  // driveLog of k_emit, src/axon.mm:216-220
@@ -520,6 +522,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       if (dbuf) cp_async_wait<1>();  // all but the copies just issued: this trajectory's
       else cp_async_wait<0>();
       if (tid == 0) { sMisc[4] = 0u; sCtl[0] = 0u; }
+      __syncthreads();  // every thread's copies have landed
       if (warp == 0) {  // drives the histogram holds
         uint32_t n = 0;
         for (uint32_t i = lane; i < kThetaBins; i += 32u) n += sH[i];
@@ -631,7 +634,8 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
 size_t recall_smem_bytes(uint32_t ncol, uint32_t B, uint32_t acc32, uint32_t dacc) {
   (void)ncol;
   const size_t stride = acc32 ? 33 : 17;
-  return (2ull * kItemWords + (dacc ? 2 : 1) * kRecallCpi * (size_t)B * stride + 2 * (64 + 68 + 68 + 68) + 16 + 4) * 4;
+  return (2ull * kItemWords + (dacc ? 2 : 1) * kRecallCpi * (size_t)B * stride + 2 * (64 + 68 + 68 + 68) + 16 + 4 + B) *
+         4;
 }
 
 namespace {
