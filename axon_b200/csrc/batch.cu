@@ -51,13 +51,13 @@ cudaError_t launch_make_w3r(const uint4* W3, uint32_t* W3R, uint32_t ncol, cudaS
 }
 
 // Row rr (= column-in-item * B + trajectory) of a counter buffer. Packed rows are 16 words
-// (32 neurons in 16-bit pairs) at a stride of 17, the odd stride spreading the rows of
-// different trajectories over the banks; each packed row starts on an even word (one word of
-// slack after even rows), so the write-back reads it in 8-byte pairs. (Adding four rows by
-// one 64-bit shared atomic was measured: 9.76 ms per benchmark batch against 7.01 ms.)
+// (32 neurons in 16-bit pairs) at a stride of 17 (32-bit rows at 33): the odd stride
+// spreads the rows of different trajectories over all 32 banks. (Rows aligned to even words
+// for 8-byte accesses leave only 16 starting banks: measured slower, as was adding four rows
+// by one 64-bit shared atomic, 9.76 ms per benchmark batch against 7.01 ms.)
 template <bool PACK>
 __device__ __forceinline__ uint32_t* acc_row(uint32_t* accB, uint32_t rr) {
-  return PACK ? accB + rr * 17u + (rr & 1u) : accB + rr * 33u;
+  return accB + rr * (PACK ? 17u : 33u);
 }
 
 // One m16n8k256 binary MMA: d = c + popcount(a AND b) over 256 bits, a 16 x 256 bit rows
@@ -432,10 +432,9 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         while (b >= B && colL < ncl) { b -= B; ++colL; }
         while (colL < ncl) {  // uniform over the four lanes of a pair
           const uint32_t col = c0 + colL;
-          uint2* src = reinterpret_cast<uint2*>(acc_row<PACK>(accB, colL * B + b) + q * 4u);
-          const uint2 w01 = src[0], w23 = src[1];
-          src[0] = src[1] = make_uint2(0u, 0u);
-          const uint4 w = make_uint4(w01.x, w01.y, w23.x, w23.y);
+          uint32_t* src = acc_row<PACK>(accB, colL * B + b) + q * 4u;
+          const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
+          src[0] = src[1] = src[2] = src[3] = 0u;
           reinterpret_cast<uint4*>(d.acc)[((size_t)b * ncol + col) * 4u + q] = w;
           // sum of the 8 per-neuron drives in w: each word is lo + 65536 hi, so lo + hi is
           // the word minus 65535 hi
