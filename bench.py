@@ -313,6 +313,16 @@ def plain_alg_bytes(hist: np.ndarray, conn: np.ndarray) -> float:
     return float((1024.0 * tiles + 512 * 1024 + 16 * 1024).sum())
 
 
+def contraction_popcounts(hist: np.ndarray, conn: np.ndarray) -> float:
+    """The AND-popcounts the batched contraction cannot avoid: per trajectory-step, for every
+    (column, branch) whose presynaptic group spiked at t-1, one 32-bit AND-popcount per row
+    (32 rows) and per nonzero spike word of the group."""
+    ngrp = NCOL // 8
+    fan = np.bincount(conn.astype(np.int64), minlength=ngrp).astype(np.float64)
+    nzw = (hist.reshape(hist.shape[0], hist.shape[1], ngrp, 8) != 0).sum(-1)  # nonzero words per group
+    return float(32.0 * (nzw[:, :-1] * fan).sum())
+
+
 def cli_args() -> list[str]:
     return [f"{k}={v}" for k, v in CONFIG_C_KEYS.items()] + ["stimcols=64", "T=10", "clampsteps=5"]
 
@@ -660,6 +670,9 @@ def main() -> None:
     spikes = 2 * B * NCOL * 4
     alg_bytes = T_RECALL * (w3_bytes + spikes)
     achieved = alg_bytes / (ms / 1e3) / 1e9
+    pops = contraction_popcounts(ref["hist"], conn)
+    sm_mhz = clk.summary().get("sm_mhz") or 1965.0
+    peak_pops = torch.cuda.get_device_properties(dev).multi_processor_count * 16 * sm_mhz * 1e6
     cpu = None if (args.no_cpu or world != 1) else cpu_sample(net, cues, ev, ref["hist"], threads, args.cpu_traj)
     line = {
         "metric": "synaptic events/s (batched recall, 300 trajectories x 45 steps)",
@@ -677,6 +690,11 @@ def main() -> None:
                      "traffic": measured_traffic("k_recall"), "peak_kind": pk,
                      "note": "algorithmic bytes = 45 x (W3 128 MiB + every trajectory's spike vector in and out); "
                              "the kernel is bound by the popcount (XU) pipe and issue, see profiles/"},
+        "int_roofline": {"bound": "xu (popcount pipe)", "achieved": pops / (ms / 1e3), "unit": "popcounts/s",
+                         "peak": peak_pops, "frac": pops / (ms / 1e3) / peak_pops,
+                         "note": "the contraction's unavoidable 32-bit AND-popcounts (32 rows x nonzero spike words "
+                                 "of every active (column, branch, trajectory)) per second, against 16 popcounts per SM "
+                                 "per clock at the sampled SM clock; ncu's XU-pipe utilisation is the same measure"},
         "cpu_baseline": cpu,
         "e2e": {"value": world * events / e2e_s, "unit": "synaptic events/s", "h2d_bytes_per_step": int(cues.nbytes),
                 "d2h_bytes_per_step": int(B * NCOL * 4)},
