@@ -105,6 +105,52 @@ __global__ void __launch_bounds__(kPresentMaxWarps * 32, 1) k_present(NetDev d, 
   }
   __syncthreads();
 
+  // what phase A leaves for phase C; readout launches keep a step's values until its records
+  // are written, during the next step's tile copies
+  uint32_t acc[CPW], bb[CPW], vk[CPW], vk1[CPW];
+#pragma unroll
+  for (int i = 0; i < CPW; ++i) acc[i] = bb[i] = vk[i] = vk1[i] = 0u;
+  // Records of column slot i for step tr, whose spike ballot is bw: the final state at the
+  // last step, stats[2] and driveLog (src/axon.mm:213-220), hist and the k_emit counters
+  // (src/axon.mm:224-234).
+  auto records = [&](int i, uint32_t tr, uint32_t bw) {
+    const uint32_t cc = col[i];
+    const uint32_t slot = warp * CPW + (uint32_t)i;
+    const bool recur = cc >= incols;
+    const bool fired = (bw >> lane) & 1u;
+    if (tr + 1u == c.T) {  // final state of the owned neurons, as present() leaves it
+      d.acc[cc * 32u + lane] = acc[i];
+      d.bbits[cc * 32u + lane] = bb[i];
+      if (lane == 0) d.marg[cc] = vk[i] > vk1[i] ? 1u : 0u;
+    }
+    if (recur) {
+      const uint32_t coinc = __reduce_add_sync(kFull, fired ? (uint32_t)__popc(bb[i]) : 0u);
+      const bool member = (sRef[slot] >> lane) & 1u;
+      const bool shared = sMul[slot * 32u + lane] > 1u;
+      const uint32_t mS = __ballot_sync(kFull, member && shared), mE = __ballot_sync(kFull, member && !shared);
+      const uint32_t sumS = __reduce_add_sync(kFull, (member && shared) ? acc[i] : 0u);
+      const uint32_t sumE = __reduce_add_sync(kFull, (member && !shared) ? acc[i] : 0u);
+      if (lane == 0) {
+        if (coinc) atomicAdd(d.stats + 2, coinc);
+        if (mS) { atomicAdd(d.driveLog + tr * 4u + 0u, sumS); atomicAdd(d.driveLog + tr * 4u + 1u, (uint32_t)__popc(mS)); }
+        if (mE) { atomicAdd(d.driveLog + tr * 4u + 2u, sumE); atomicAdd(d.driveLog + tr * 4u + 3u, (uint32_t)__popc(mE)); }
+      }
+    }
+    if (lane == 0) {
+      d.hist[(size_t)tr * ncol + cc] = bw;
+      if (bw != 0u && recur) {
+        const uint32_t sb = 64u + tr * 8u;
+        atomicAdd(d.stats + 0, 1u);
+        atomicAdd(d.stats + 1, (uint32_t)__popc(bw));
+        atomicAdd(d.stats + sb + 0u, vk[i] - vk1[i]);
+        atomicAdd(d.stats + sb + 1u, vk[i]);
+        atomicAdd(d.stats + sb + 2u, 1u);
+        if (vk[i] == vk1[i]) atomicAdd(d.stats + sb + 3u, 1u);
+        if (vk[i] == 0u) atomicAdd(d.stats + sb + 4u, 1u);
+      }
+    }
+  };
+
   for (uint32_t t = 0; t < c.T; ++t) {
     const uint32_t* sIn = (t & 1u) ? sSpk1 : sSpk0;
     uint32_t* sOut = (t & 1u) ? sSpk0 : sSpk1;
@@ -115,10 +161,10 @@ __global__ void __launch_bounds__(kPresentMaxWarps * 32, 1) k_present(NetDev d, 
     const bool clamp = t < c.clampSteps;
     const uint32_t phase = (!LEARN || !c.contrast) ? 0u
                            : (clamp ? 1u : (((t - c.clampSteps) % c.ltdEvery == 0u) ? 2u : 3u));
-    // what phase A leaves for phase C of the same step
-    uint32_t acc[CPW], bb[CPW], vk[CPW], vk1[CPW];
+    if (LEARN) {
 #pragma unroll
-    for (int i = 0; i < CPW; ++i) acc[i] = bb[i] = vk[i] = vk1[i] = 0u;
+      for (int i = 0; i < CPW; ++i) acc[i] = bb[i] = vk[i] = vk1[i] = 0u;
+    }
 
     // per-phase device timer stamps of the profile mode (thread 0 of every CTA)
     unsigned long long* stamp = d.prof ? d.prof + ((size_t)t * gridDim.x + blockIdx.x) * 5u : nullptr;
@@ -139,8 +185,9 @@ __global__ void __launch_bounds__(kPresentMaxWarps * 32, 1) k_present(NetDev d, 
       uint32_t slot0 = 0;
       if (lane == 0 && n != 0u) slot0 = atomicAdd(sFlag + 3, n);
       slot0 = __shfl_sync(kFull, slot0, 0);
-      if (n != 0u && slot0 + n <= poolTiles) {
-        uint64_t* mb = &sMbar[warp * CPW + (uint32_t)i];
+      const bool pooled = n != 0u && slot0 + n <= poolTiles;
+      uint64_t* mb = &sMbar[warp * CPW + (uint32_t)i];
+      if (pooled) {
         if (lane == 0) mbar_expect_tx(mb, n * 1024u);
         __syncwarp();
         if (on) {
@@ -148,6 +195,13 @@ __global__ void __launch_bounds__(kPresentMaxWarps * 32, 1) k_present(NetDev d, 
           fence_proxy_async_smem();
           bulk_g2s(sPool + (size_t)(slot0 + r) * kTileU4, d.W3 + ((size_t)cc * kNslot + lane) * kTileU4, 1024u, mb);
         }
+      }
+      // a readout writes the previous step's records while this step's tiles are in flight
+      if (!LEARN) {
+        if (t > 0u) records(i, t - 1u, sIn[cc]);
+        acc[i] = bb[i] = vk[i] = vk1[i] = 0u;
+      }
+      if (pooled) {
         const uint32_t ph = (mph >> i) & 1u;
         if (!mbar_wait(mb, ph, c.waitNs)) {
           // the copies did not land in time: record it, wait (bounded) for them, and let
@@ -259,39 +313,8 @@ __global__ void __launch_bounds__(kPresentMaxWarps * 32, 1) k_present(NetDev d, 
       const uint32_t b = sOut[cc];
       const bool recur = cc >= incols;
       const bool fired = (b >> lane) & 1u;
-      if (t + 1u == c.T) {  // final state of the owned neurons, as present() leaves it
-        d.acc[cc * 32u + lane] = acc[i];
-        d.bbits[cc * 32u + lane] = bb[i];
-        if (lane == 0) d.marg[cc] = vk[i] > vk1[i] ? 1u : 0u;
-      }
-      if (recur) {
-        // stats[2] and driveLog, src/axon.mm:213-220
-        const uint32_t coinc = __reduce_add_sync(kFull, fired ? (uint32_t)__popc(bb[i]) : 0u);
-        const bool member = (sRef[slot] >> lane) & 1u;
-        const bool shared = sMul[slot * 32u + lane] > 1u;
-        const uint32_t mS = __ballot_sync(kFull, member && shared), mE = __ballot_sync(kFull, member && !shared);
-        const uint32_t sumS = __reduce_add_sync(kFull, (member && shared) ? acc[i] : 0u);
-        const uint32_t sumE = __reduce_add_sync(kFull, (member && !shared) ? acc[i] : 0u);
-        if (lane == 0) {
-          if (coinc) atomicAdd(d.stats + 2, coinc);
-          if (mS) { atomicAdd(d.driveLog + t * 4u + 0u, sumS); atomicAdd(d.driveLog + t * 4u + 1u, (uint32_t)__popc(mS)); }
-          if (mE) { atomicAdd(d.driveLog + t * 4u + 2u, sumE); atomicAdd(d.driveLog + t * 4u + 3u, (uint32_t)__popc(mE)); }
-        }
-      }
-      if (lane == 0) {
-        d.hist[(size_t)t * ncol + cc] = b;
-        if (b != 0u && recur) {  // src/axon.mm:225-234
-          const uint32_t sb = 64u + t * 8u;
-          atomicAdd(d.stats + 0, 1u);
-          atomicAdd(d.stats + 1, (uint32_t)__popc(b));
-          atomicAdd(d.stats + sb + 0u, vk[i] - vk1[i]);
-          atomicAdd(d.stats + sb + 1u, vk[i]);
-          atomicAdd(d.stats + sb + 2u, 1u);
-          if (vk[i] == vk1[i]) atomicAdd(d.stats + sb + 3u, 1u);
-          if (vk[i] == 0u) atomicAdd(d.stats + sb + 4u, 1u);
-        }
-      }
-      if (!LEARN) continue;
+      if (!LEARN) continue;  // a readout's records wait for the next step's tile copies
+      records(i, t, b);
       // k_bias, src/axon.mm:240-253
       if (recur) {
         const int dec = ((t % max(c.biasDownEvery, 1u)) == 0u) ? (int)c.biasDown : 0;
@@ -370,6 +393,11 @@ __global__ void __launch_bounds__(kPresentMaxWarps * 32, 1) k_present(NetDev d, 
   // ---------------- final state, as the reference's buffers hold it after present()
   const uint32_t T = c.T;
   const uint32_t* sLast = (T & 1u) ? sSpk1 : sSpk0;   // spk(T-1)
+  if (!LEARN) {  // the last step's records
+#pragma unroll
+    for (int i = 0; i < CPW; ++i)
+      if (col[i] < ncol) records(i, T - 1u, sLast[col[i]]);
+  }
   const uint32_t* sPrev = (T & 1u) ? sSpk0 : sSpk1;   // spk(T-2), zero when T == 1
   uint32_t* gLast = ((T - 1u) & 1u) ? d.spkA : d.spkB;
   uint32_t* gPrev = ((T - 1u) & 1u) ? d.spkB : d.spkA;
