@@ -69,7 +69,10 @@ __global__ void __launch_bounds__(kPresentMaxWarps * 32, 1) k_present(NetDev d, 
   uint32_t* sB = sD + ncol;                // staged ungated ballots
   uint32_t* sCand = sB + ncol;             // drives of the threshold's histogram bin (up to ncol)
 
-  const uint32_t gwarp = blockIdx.x * wpb + warp, nwarps = gridDim.x * wpb;
+  // columns are dealt to warps CTA-interleaved (column = warp * grid + CTA): the clamped
+  // input columns, which all fire and learn during the clamp, spread over every CTA instead
+  // of loading the first few
+  const uint32_t gwarp = warp * gridDim.x + blockIdx.x, nwarps = gridDim.x * wpb;
   uint32_t* xhist = d.bar + 64;            // step t counts its recurrent drives into histogram t mod 3
   // branch term of k_drive (src/axon.mm:174-178): the count (modes 0, 1) plus, when the
   // branch reaches dthr, the boost (mode 1) or 1 (mode 2)
