@@ -121,3 +121,16 @@ def test_table1_row_regenerated(stim):
     assert f"{float(m['within_pct']):.2f}" == row["within"]
     assert (m["recall"], m["best_other"], m["margin"], m["sustained"], m["drive_t6"]) == (
         row["recall"], row["best_other"], row["margin"], row["sustained"], row["drive"])
+
+
+def test_table2_fixture_matches_paper():
+    """The oracle's five-seed runs (tests/golden/oracle_table2.json, made by make_golden.py),
+    summarised as bench/seeds.sh summarises them, reproduce the published replication
+    table (paper/axon_preprint.tex:288-292) and its 12-pattern sustained mean (:298-299)."""
+    fx = json.loads((Path(__file__).parent / "golden" / "oracle_table2.json").read_text())
+    t2 = GOLD["table2"]
+    for row in t2["rows"]:
+        got = fx["summary"][str(row["stim"])]
+        for f in ("sustained_mean", "sustained_sd", "margin_mean", "margin_sd", "within_mean", "within_sd"):
+            assert got[f] == row[f], (row["stim"], f, got[f], row[f])
+    assert fx["summary"]["12"]["sustained_mean"] == t2["stim12_sustained_mean"]
