@@ -236,14 +236,18 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   };
   // warp 0: the item's branch groups and the prefixes of its 64 entry-list lengths, single-
   // word and multi-word, into buffer buf
+  // groups below skipGroups contribute nothing this step: their entries are left out (the
+  // clamped input groups while their contribution comes from the afferent cache)
+  uint32_t skipGroups = 0;
   auto prep = [&](uint32_t item, uint32_t buf, const uint32_t* c1In, const uint32_t* cMIn) {
     const uint32_t c0 = item * kRecallCpi;
     const bool v1 = c0 + 1 < ncol;
     const uint32_t g0 = __ldg(d.conn + c0 * kNslot + lane), g1 = v1 ? __ldg(d.conn + (c0 + 1) * kNslot + lane) : 0u;
     sConn[buf * 64u + lane] = g0;
     sConn[buf * 64u + 32u + lane] = g1;
-    uint32_t a0 = __ldcg(c1In + g0), a1 = v1 ? __ldcg(c1In + g1) : 0u;
-    uint32_t m0 = __ldcg(cMIn + g0), m1 = v1 ? __ldcg(cMIn + g1) : 0u;
+    const bool u0 = g0 >= skipGroups, u1 = v1 && g1 >= skipGroups;
+    uint32_t a0 = u0 ? __ldcg(c1In + g0) : 0u, a1 = u1 ? __ldcg(c1In + g1) : 0u;
+    uint32_t m0 = u0 ? __ldcg(cMIn + g0) : 0u, m1 = u1 ? __ldcg(cMIn + g1) : 0u;
     uint32_t k0 = (a0 + m0 + 7u) >> 3, k1 = (a1 + m1 + 7u) >> 3;  // MMA chunks of the branch
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -285,6 +289,14 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     uint32_t* c1Out = d.ecnt + (size_t)(par ^ 1u) * 2 * ngrp;
     uint32_t* cMOut = c1Out + ngrp;
     const bool clamp = t < c.clampSteps;
+    // Afferent cache. While the inputs are clamped their spike words are the cue in every
+    // step, so the input groups' dendritic terms are the same at steps 1..clampSteps: step 1
+    // (whose drives come from the input groups alone, every recurrent column being silent at
+    // step 0) stores its per-neuron counters, and steps 2..clampSteps leave the input groups'
+    // entries out and add the stored counters in the write-back.
+    const bool affStore = d.aff != nullptr && t == 1u;
+    const bool affAdd = d.aff != nullptr && t >= 2u && t <= c.clampSteps;
+    skipGroups = affAdd ? incols / 8u : 0u;
 
     // next step's list lengths start at zero (last read in phase 1 of step t-1)
     if (blockIdx.x == 0)
@@ -433,8 +445,17 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         while (colL < ncl) {  // uniform over the four lanes of a pair
           const uint32_t col = c0 + colL;
           uint32_t* src = acc_row<PACK>(accB, colL * B + b) + q * 4u;
-          const uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
+          uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
           src[0] = src[1] = src[2] = src[3] = 0u;
+          if (affStore || affAdd) {  // the afferent cache (halves add without carry: drives stay below 2^16)
+            uint4* ap = reinterpret_cast<uint4*>(d.aff) + ((size_t)b * ncol + col) * 4u + q;
+            if (affStore) {
+              __stcg(ap, w);
+            } else {
+              const uint4 a = __ldcg(ap);
+              w.x += a.x; w.y += a.y; w.z += a.z; w.w += a.w;
+            }
+          }
           reinterpret_cast<uint4*>(d.acc)[((size_t)b * ncol + col) * 4u + q] = w;
           // sum of the 8 per-neuron drives in w: each word is lo + 65536 hi, so lo + hi is
           // the word minus 65535 hi
