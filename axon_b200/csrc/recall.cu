@@ -141,9 +141,10 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     const size_t bnc = (size_t)Bc * ncol;
     const size_t accBytes = bnc * 32 * (rc.acc32 ? 4 : 2);
     // the afferent cache of the clamped steps: the packed counters' fast write-back path only
-    // (no bias, facilitation or drive log), when steps 2.. are clamped
+    // (no bias, facilitation or drive log), when steps 2.. are clamped and the input columns
+    // fill whole groups (a group holding input and recurrent columns changes while clamped)
     const bool useAff = !rc.acc32 && !rc.useBias && rc.facil == 0u && dRef == nullptr && a.clamp_steps >= 2u &&
-                        a.T >= 3u;
+                        a.T >= 3u && cfg.incols % 8u == 0u;
     const size_t affBytes = useAff ? bnc * 16 * 4 : 0;
     const size_t need = al(2 * bnc * 4) + al(2ull * ngrp * Bc * 8) + al(2ull * ngrp * Bc * 16) + al(4ull * ngrp * 4) + al(bnc * 4) +
                         al(accBytes) + al((size_t)std::max(a.T, 64u) * 4) + al(3ull * Bc * kHistWords * 4) + al((size_t)Bc * 4) +

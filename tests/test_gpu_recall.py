@@ -71,7 +71,7 @@ def test_recall_matches_oracle_small(method, B, T, clamp, use_bias):
 
 
 @pytest.mark.parametrize("variant", [dict(mode=0, dthr=2), dict(mode=2, dthr=0, boost=9), dict(ktest=5, facil=40),
-                                     dict(topkpar=0, target=0), dict(target=300), dict(boost=2000)])
+                                     dict(topkpar=0, target=0), dict(target=300), dict(boost=2000), dict(incols=20)])
 def test_recall_variants(variant):
     cfg, gpu, cpu, pats = trained_pair(variant, 4, 2, 16)
     cues = make_cues(pats, cfg.ncol, 9, np.random.default_rng(0))
