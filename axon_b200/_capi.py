@@ -33,11 +33,12 @@ class AxonCfg(C.Structure):
 
 class RecallArgs(C.Structure):
     _fields_ = [("T", C.c_uint32), ("clamp_steps", C.c_uint32), ("use_bias", C.c_uint32), ("method", C.c_uint32),
-                ("graph", C.c_uint32), ("contraction", C.c_uint32), ("reserved", C.c_uint32 * 2)]
+                ("graph", C.c_uint32), ("contraction", C.c_uint32), ("slab", C.c_uint32), ("reserved", C.c_uint32 * 1)]
 
 
 RECALL_BATCHED, RECALL_PLAIN = 0, 1
 CONTRACT_POPC, CONTRACT_TENSOR = 0, 1
+SLAB = {"floor": 0, "floor_always": 1, "full": 2}
 
 STATE_DEV_FIELDS = ["w0", "w1", "w2", "w3", "conn", "bias", "mult", "refball", "stim", "spk_a", "spk_b", "drive",
                     "bbits", "acc", "marg", "drive_log", "stats", "hist", "theta"]

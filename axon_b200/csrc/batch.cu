@@ -183,6 +183,47 @@ static __device__ __noinline__ uint32_t recall_theta(const uint32_t* sD, const u
   return hist_theta<-1>(sD, sH, sCand, sCtl, incols, ncol, need, topkPar);
 }
 
+// The per-neuron drives of column cc for one trajectory, recomputed from that trajectory's
+// spike vector of the previous step (spkB, ncol words), for a gated column whose entry the
+// write-back did not store. Lane = branch: its group's nonzero spike words AND-counted
+// against the branch's 32 tile rows give its 32 dendritic terms, none for a silent group
+// (src/axon.mm:166-178, the terms the phase-1 units add); the lanes add them into the
+// warp's 32 row sums in shared memory (scr, zero on entry and on return), and lane r
+// returns neuron r's drive. Loops over rows are not unrolled: the path is rare, and its
+// registers count against the whole kernel's.
+template <bool LIN>
+__device__ __forceinline__ uint32_t recompute_drive(const uint32_t* W3R, const uint32_t* conn, const uint32_t* spkB,
+                                                    uint32_t cc, uint32_t dthr, uint32_t bst, uint32_t lane,
+                                                    uint32_t* scr) {
+  const uint32_t g = __ldg(conn + cc * kNslot + lane);
+  const uint4 p = __ldcg(reinterpret_cast<const uint4*>(spkB + 8u * g));
+  const uint4 q = __ldcg(reinterpret_cast<const uint4*>(spkB + 8u * g) + 1);
+  const uint32_t S[8] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w};
+  if ((p.x | p.y | p.z | p.w | q.x | q.y | q.z | q.w) != 0u) {
+    const uint32_t* tile = W3R + (size_t)cc * kColWords + lane * 256u;
+#pragma unroll 1
+    for (uint32_t r = 0; r < 32u; r += 4) {
+      uint32_t c0 = 0u, c1 = 0u, c2 = 0u, c3 = 0u;
+#pragma unroll
+      for (uint32_t w = 0; w < 8u; ++w) {
+        if (S[w] == 0u) continue;
+        const uint4 a = __ldg(reinterpret_cast<const uint4*>(tile + w3r_pos(r, w)));
+        c0 += __popc(a.x & S[w]); c1 += __popc(a.y & S[w]);
+        c2 += __popc(a.z & S[w]); c3 += __popc(a.w & S[w]);
+      }
+      atomicAdd(scr + r, branch_term<LIN>(c0, dthr, bst));
+      atomicAdd(scr + r + 1u, branch_term<LIN>(c1, dthr, bst));
+      atomicAdd(scr + r + 2u, branch_term<LIN>(c2, dthr, bst));
+      atomicAdd(scr + r + 3u, branch_term<LIN>(c3, dthr, bst));
+    }
+  }
+  __syncwarp();
+  const uint32_t a = scr[lane];
+  scr[lane] = 0u;
+  __syncwarp();
+  return a;
+}
+
 // MMA: the AND-popcount contraction of phase 1 on the tensor cores (mma.sync b1 and.popc,
 // m16n8k256: 16 tile rows x 8 entries x the group's 256 spike bits per instruction) instead
 // of __popc on the CUDA cores; the dendritic terms, counters and everything else are shared.
@@ -297,6 +338,15 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     const bool affStore = d.aff != nullptr && t == 1u;
     const bool affAdd = d.aff != nullptr && t >= 2u && t <= c.clampSteps;
     skipGroups = affAdd ? incols / 8u : 0u;
+    // Sparse drive slab (packed path without bias, facilitation or drive log): the write-back
+    // stores a (column, trajectory) entry only when the column drive reaches the trajectory's
+    // histogram floor. A threshold selected from the histogram is at least the floor, so every
+    // gated column has its entry; after a sorting fallback, phase 2 recomputes the gated
+    // columns below the floor. At the first step after the clamp the drives fall below the
+    // floor for almost every trajectory, so the host has that step store every entry
+    // (slabAllStep), or every step (slabFull).
+    const bool fast = PACK && !c.useBias && c.facil == 0u && d.refBall == nullptr;
+    const bool storeAll = c.slabFull != 0u || t == c.slabAllStep;
 
     // next step's list lengths start at zero (last read in phase 1 of step t-1)
     if (blockIdx.x == 0)
@@ -432,7 +482,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       }
       if (tid == 0) sMisc[6 + bcur] = 0u;  // every warp has claimed its units of this item
       // per-neuron and column drives of the item's columns for every trajectory
-      if (PACK && !c.useBias && !c.facil && d.refBall == nullptr) {
+      if (fast) {
         // the packed counters already are the u16 drive slab: four lanes per (column,
         // trajectory), each storing 4 of its 16 words as one 16-byte vector
         // (column, trajectory) pairs in column-major order: the trajectory index steps by
@@ -456,17 +506,17 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
               w.x += a.x; w.y += a.y; w.z += a.z; w.w += a.w;
             }
           }
-          reinterpret_cast<uint4*>(d.acc)[((size_t)b * ncol + col) * 4u + q] = w;
           // sum of the 8 per-neuron drives in w: each word is lo + 65536 hi, so lo + hi is
           // the word minus 65535 hi
           uint32_t s = (w.x - 65535u * (w.x >> 16)) + (w.y - 65535u * (w.y >> 16)) + (w.z - 65535u * (w.z >> 16)) +
                        (w.w - 65535u * (w.w >> 16));
           s += __shfl_xor_sync(gmask, s, 1);
           s += __shfl_xor_sync(gmask, s, 2);
+          const uint32_t fl = sFloor[b];
+          if (storeAll || s >= fl) reinterpret_cast<uint4*>(d.acc)[((size_t)b * ncol + col) * 4u + q] = w;
           if (q == 0) {
             __stcg(d.drv + (size_t)b * ncol + col, s);
-            if (col >= incols && s >= sFloor[b])
-              count_drive(d.thHist + ((size_t)(t % 3u) * B + b) * kHistWords, s);
+            if (col >= incols && s >= fl) count_drive(d.thHist + ((size_t)(t % 3u) * B + b) * kHistWords, s);
           }
           b += nw * 8u;
           while (b >= B && colL < ncl) { b -= B; ++colL; }
@@ -515,9 +565,10 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     // The column drives and the drive histogram of the CTA's trajectories arrive by
     // asynchronous copies; with two buffers the next trajectory's copies are in flight while
     // the current one is processed.
-    const bool dbuf = 4u * ncol + 512u + 2u * kHistWords <= 2u * kItemWords;
+    const bool dbuf = 4u * ncol + 512u + 2u * kHistWords + 32u * nw <= 2u * kItemWords;
     uint32_t* const sD1 = sH0 + kHistWords;
     uint32_t* const sH1 = sD1 + ncol;
+    uint32_t* const sScr = (dbuf ? sH1 : sH0) + kHistWords + 32u * warp;  // [nw][32] drive recompute sums
     const uint32_t* hStep = d.thHist + (size_t)(t % 3u) * B * kHistWords;
     auto load_drv = [&](uint32_t b, uint32_t slot) {
       const uint4* src = reinterpret_cast<const uint4*>(d.drv + (size_t)b * ncol);
@@ -561,6 +612,8 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         if (lane == 0) sCtl[8] = n;
       }
       __syncthreads();
+      // gated columns whose drive is below reFloor have no slab entry (a fallback select)
+      const uint32_t reFloor = fast && !storeAll && sCtl[8] < c.targetCols ? sFloor[b] : 0u;
       const uint32_t theta = sCtl[8] >= c.targetCols
                                  ? recall_theta(sD, sH, sList, sCtl, incols, ncol, c.targetCols, c.topkPar)
                                  : block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed,
@@ -581,7 +634,37 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       }
       __syncthreads();
       const uint32_t npend = sMisc[4];
-      // a warp's gated columns kPend at a time: their per-neuron drives load together
+      // k-of-32 of one gated column from its per-neuron drive a (one per lane)
+      auto emit_col = [&](uint32_t cc, uint32_t a) {
+        uint32_t vk, vk1;
+        const uint32_t ball = warp_kwta(a, lane, c.k, vk, vk1);
+        if (lane == 0) {
+          sSpk[cc] = ball;
+          if (d.stats && ball != 0u && cc >= incols) {  // k_emit counters, src/axon.mm:225-234
+            uint32_t* st = d.stats + (size_t)b * 1024u;
+            const uint32_t sb = 64u + t * 8u;
+            atomicAdd(st + 0, 1u);
+            atomicAdd(st + 1, (uint32_t)__popc(ball));
+            atomicAdd(st + sb + 0u, vk - vk1);
+            atomicAdd(st + sb + 1u, vk);
+            atomicAdd(st + sb + 2u, 1u);
+            if (vk == vk1) atomicAdd(st + sb + 3u, 1u);
+            if (vk == 0u) atomicAdd(st + sb + 4u, 1u);
+          }
+        }
+      };
+      // gated columns without a slab entry: drives recomputed, one column per warp
+      if (reFloor != 0u) {
+        sScr[lane] = 0u;
+        __syncwarp();
+        for (uint32_t e = warp; e < npend; e += nw) {
+          const uint32_t cc = sList[e];
+          if (sD[cc] < reFloor)
+            emit_col(cc, recompute_drive<LIN>(d.W3R, d.conn, spkIn + (size_t)b * ncol, cc, dthr, bst, lane, sScr));
+        }
+      }
+      // the others from the slab, a warp's gated columns kPend at a time: their per-neuron
+      // drives load together
       constexpr uint32_t kPend = 4;
       for (uint32_t e0 = warp; e0 < npend; e0 += kPend * nw) {
         uint32_t av[kPend];
@@ -589,7 +672,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         for (uint32_t u = 0; u < kPend; ++u) {
           const uint32_t e = e0 + u * nw;
           av[u] = 0u;
-          if (e < npend) {
+          if (e < npend && sD[sList[e]] >= reFloor) {
             const size_t o = ((size_t)b * ncol + sList[e]) * 32u + lane;
             av[u] = c.acc32 ? __ldcg(reinterpret_cast<const uint32_t*>(d.acc) + o)
                             : (uint32_t)__ldcg(reinterpret_cast<const uint16_t*>(d.acc) + o);
@@ -600,23 +683,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
           const uint32_t e = e0 + u * nw;
           if (e >= npend) break;  // warp-uniform
           const uint32_t cc = sList[e];
-          const uint32_t a = av[u];
-          uint32_t vk, vk1;
-          const uint32_t ball = warp_kwta(a, lane, c.k, vk, vk1);
-          if (lane == 0) {
-            sSpk[cc] = ball;
-            if (d.stats && ball != 0u && cc >= incols) {  // k_emit counters, src/axon.mm:225-234
-              uint32_t* st = d.stats + (size_t)b * 1024u;
-              const uint32_t sb = 64u + t * 8u;
-              atomicAdd(st + 0, 1u);
-              atomicAdd(st + 1, (uint32_t)__popc(ball));
-              atomicAdd(st + sb + 0u, vk - vk1);
-              atomicAdd(st + sb + 1u, vk);
-              atomicAdd(st + sb + 2u, 1u);
-              if (vk == vk1) atomicAdd(st + sb + 3u, 1u);
-              if (vk == 0u) atomicAdd(st + sb + 4u, 1u);
-            }
-          }
+          if (sD[cc] >= reFloor) emit_col(cc, av[u]);
         }
       }
       __syncthreads();

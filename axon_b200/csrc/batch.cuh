@@ -23,7 +23,9 @@ struct RecallDev {
   uint4* entM;              // [2][ngrp][B] per-group lists of trajectories with several nonzero words
   uint32_t* ecnt;           // [2 parity][2 lists][ngrp] list lengths (parity 0 zeroed before launch)
   uint32_t* drv;            // [B][ncol] column drives of the current step
-  void* acc;                // [B][ncol][32] per-neuron drive (u16 or u32) of the current step
+  void* acc;                // [B][ncol][32] per-neuron drive (u16 or u32) of the current step; on the packed
+                            // path without bias, facilitation or drive log only the entries whose column
+                            // drive reaches the trajectory's histogram floor are written
   uint32_t* finalOut;       // [B][ncol] spikes of the last step, or null
   uint32_t* hist;           // [B][T][ncol] spikes of every step, or null
   uint32_t* stats;          // [B][1024] counters (zeroed before launch), or null
@@ -43,6 +45,8 @@ struct RecallCfg {
   uint32_t bst;    // dendritic bonus per branch at or above dthr: boost (mode 1), 0 (mode 0)
   uint32_t dacc;   // 1: two counter buffers (alternating items), when they fit in shared memory
   uint32_t mma;    // 1: phase-1 AND-popcounts on the tensor cores (binary MMA), 0: __popc on the CUDA cores
+  uint32_t slabFull;     // 1: the write-back stores every per-neuron drive (packed path)
+  uint32_t slabAllStep;  // the step at which it stores every one anyway (0xFFFFFFFF: none)
   uint64_t waitNs;
 };
 

@@ -62,8 +62,8 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
   if (a.T == 0 || a.T > (records ? 64u : kRecallMaxT))
     return set_error(AXON_EINVAL, records ? "T must be in 1..64 (per-step records or the plain method)"
                                           : "T must be in 1..1024");
-  if (a.use_bias > 1 || a.method > 1 || a.contraction > 1)
-    return set_error(AXON_EINVAL, "bad use_bias, method or contraction");
+  if (a.use_bias > 1 || a.method > 1 || a.contraction > 1 || a.slab > AXON_SLAB_FULL)
+    return set_error(AXON_EINVAL, "bad use_bias, method, contraction or slab");
   CK(cudaSetDevice(device));
 
   // ---- device views of the caller's arrays (copied in when they are host arrays)
@@ -136,6 +136,8 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     rc.acc32 = maxAcc > 65535ull ? 1u : 0u;
     rc.bst = cfg.mode == 1 ? cfg.boost : 0u;
     rc.mma = a.contraction == AXON_CONTRACT_TENSOR ? 1u : 0u;
+    rc.slabAllStep = a.slab == AXON_SLAB_FLOOR ? a.clamp_steps + 1u : 0xFFFFFFFFu;
+    rc.slabFull = a.slab == AXON_SLAB_FULL ? 1u : 0u;
     const uint32_t maxB = rc.acc32 ? 300u : kRecallMaxB;
     const uint32_t Bc = std::min(B, maxB);  // trajectories per launch
     const size_t bnc = (size_t)Bc * ncol;
@@ -182,7 +184,7 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     // everything the launches depend on: a captured graph is replayed only for the same key
     const std::vector<uint64_t> key = {(uint64_t)dCues, (uint64_t)dRef, (uint64_t)dFinal, (uint64_t)dHist,
                                        (uint64_t)dStats, (uint64_t)dLog, (uint64_t)scratch.p, (uint64_t)w3b, B, a.T,
-                                       a.clamp_steps, a.use_bias, (uint64_t)rs.grid, wait_ns, a.contraction};
+                                       a.clamp_steps, a.use_bias, (uint64_t)rs.grid, wait_ns, a.contraction, a.slab};
     const bool graph = a.graph != 0u;
     const bool replay = graph && recallGraph && key == recallKey;
     if (graph && !replay) {

@@ -118,11 +118,15 @@ class Network:
     def recall(self, cues: np.ndarray, T: int, clamp_steps: int, use_bias: int = 0, method: str = "batched",
                hist: bool = False, stats: bool = False, ref_ball: np.ndarray | None = None,
                drive_log: np.ndarray | None = None, graph: bool = False, final_out: np.ndarray | None = None,
-               contraction: str = "popc") -> dict:
+               contraction: str = "popc", slab: str = "floor") -> dict:
         """B readout trajectories (present() with learn=0 for each cue row) in one call.
 
         contraction: "popc" (CUDA cores) or "tensor" (binary MMA) computes the batched
         method's AND-popcounts; the results are the same.
+        slab: which per-neuron drives the batched method stores for the k-of-32 of gated
+        columns: "floor" (columns at or above the trajectory's histogram floor, all of them
+        at the step after the clamp), "floor_always" or "full"; gated columns without a
+        stored drive are recomputed, and the results are the same.
 
         Returns {"final": (B, ncol), "hist": (B, T, ncol) | None, "stats": (B, 1024) | None,
         "drive_log": (B, 256) | None, "gpu_ms": float}. final_out, a C-contiguous uint32
@@ -134,7 +138,8 @@ class Network:
         assert cues.shape == (B, self.ncol)
         a = A.RecallArgs(T=T, clamp_steps=clamp_steps, use_bias=use_bias,
                          method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN, graph=int(graph),
-                         contraction=A.CONTRACT_TENSOR if contraction == "tensor" else A.CONTRACT_POPC)
+                         contraction=A.CONTRACT_TENSOR if contraction == "tensor" else A.CONTRACT_POPC,
+                         slab=A.SLAB[slab])
         if final_out is not None:
             assert final_out.dtype == np.uint32 and final_out.shape == (B, self.ncol) and final_out.flags.c_contiguous
         out = {"final": final_out if final_out is not None else np.empty((B, self.ncol), dtype=np.uint32),
@@ -157,12 +162,13 @@ class Network:
 
     def recall_device(self, cues_ptr: int, B: int, T: int, clamp_steps: int, final_ptr: int | None = None,
                       use_bias: int = 0, method: str = "batched", graph: bool = False,
-                      contraction: str = "popc") -> float:
+                      contraction: str = "popc", slab: str = "floor") -> float:
         """Device-resident variant: cues/final are device addresses on this network's GPU.
         graph=True replays a captured CUDA graph of the launch while the arguments repeat."""
         a = A.RecallArgs(T=T, clamp_steps=clamp_steps, use_bias=use_bias,
                          method=A.RECALL_BATCHED if method == "batched" else A.RECALL_PLAIN, graph=int(graph),
-                         contraction=A.CONTRACT_TENSOR if contraction == "tensor" else A.CONTRACT_POPC)
+                         contraction=A.CONTRACT_TENSOR if contraction == "tensor" else A.CONTRACT_POPC,
+                         slab=A.SLAB[slab])
         ms = C.c_double()
         A.check(A.lib().axon_recall_device(self._h, C.c_void_p(cues_ptr), B, C.byref(a), None,
                                            None if final_ptr is None else C.c_void_p(final_ptr), None, None, None,

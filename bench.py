@@ -503,7 +503,7 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def time_device(net, d_cues, B, T, clamp, d_final, flush, steps, contraction="popc") -> list[float]:
+def time_device(net, d_cues, B, T, clamp, d_final, flush, steps, contraction="popc", slab="floor") -> list[float]:
     import torch
 
     times = []
@@ -511,7 +511,7 @@ def time_device(net, d_cues, B, T, clamp, d_final, flush, steps, contraction="po
         flush.zero_()  # evict L2 between timed steps (untimed: outside the device-timed launch)
         torch.cuda.synchronize()
         times.append(net.recall_device(d_cues.data_ptr(), B, T, clamp, d_final.data_ptr(), graph=True,
-                                       contraction=contraction))
+                                       contraction=contraction, slab=slab))
     torch.cuda.synchronize()
     return times
 
@@ -606,7 +606,7 @@ def main() -> None:
         assert np.array_equal(r["final"], ref["final"])
     e2e_s = rep.max(float(np.mean(e2e_t)) if e2e_t else float("nan"))
 
-    wave = contraction = None
+    wave = contraction = slab = None
     if not args.no_ab:
         # the reference-parity variant: the wave readout's 5 clamped + 30 free steps
         rw = net.recall(cues, T_WAVE, CLAMP_WAVE, hist=True, contraction=ctr)
@@ -637,6 +637,17 @@ def main() -> None:
                        "faster": min(per, key=per.get),
                        "note": "tensor = mma.sync m16n8k256 b1 and.popc, 8 entries x 32 rows per chunk; popc = __popc "
                                "on the CUDA cores"}
+        # A/B of the drive slab: every per-neuron drive stored (full) against only those at or
+        # above each trajectory's histogram floor (the default)
+        rf = net.recall(cues, T_RECALL, CLAMP_RECALL, hist=True, contraction=ctr, slab="full")
+        full_exact = bool(np.array_equal(rf["hist"], ref["hist"]))
+        for _ in range(args.warmup):
+            net.recall_device(d_cues.data_ptr(), B, T_RECALL, CLAMP_RECALL, d_fw.data_ptr(), graph=True,
+                              contraction=ctr, slab="full")
+        tf = time_device(net, d_cues, B, T_RECALL, CLAMP_RECALL, d_fw, flush, max(5, args.steps // 2), ctr, "full")
+        slab = {"floor_ms_per_step": ms, "full_ms_per_step": rep.max(float(np.mean(tf))), "full_bit_exact": full_exact,
+                "note": "floor = per-neuron drives stored for columns at or above the trajectory's histogram floor "
+                        "(all at the step after the clamp; gated columns without one recomputed); full = all stored"}
 
     # plain GPU path on the same 300 trajectories (one persistent launch per trajectory)
     plain = None
@@ -700,6 +711,7 @@ def main() -> None:
                 "d2h_bytes_per_step": int(B * NCOL * 4)},
         "wave_variant": wave,
         "contraction_ab": contraction,
+        "slab_ab": slab,
         "plain": plain,
         "batched_over_plain": (value / plain["value"]) if plain else None,
         "plain_train": ptrain,

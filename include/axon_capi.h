@@ -178,10 +178,19 @@ typedef struct axon_recall_args {
                            (src/axon.mm:166-173): AXON_CONTRACT_POPC (0, __popc on the CUDA
                            cores) or AXON_CONTRACT_TENSOR (1, binary MMA on the tensor cores);
                            the results are the same */
-  uint32_t reserved[2]; /* zero */
+  uint32_t slab;        /* batched method, 16-bit counters without bias or facilitation: which
+                           per-neuron drives the kernel stores for the k-of-32 of the columns
+                           that pass the gate. AXON_SLAB_FLOOR (0): those of columns whose
+                           drive reaches the trajectory's threshold-histogram floor (half its
+                           previous threshold), and every one at the step after the clamp;
+                           AXON_SLAB_FLOOR_ALWAYS (1): the floor at every step; AXON_SLAB_FULL
+                           (2): every one. A gated column without a stored drive has it
+                           recomputed; the results are the same */
+  uint32_t reserved[1]; /* zero */
 } axon_recall_args;
 
 enum { AXON_CONTRACT_POPC = 0, AXON_CONTRACT_TENSOR = 1 };
+enum { AXON_SLAB_FLOOR = 0, AXON_SLAB_FLOOR_ALWAYS = 1, AXON_SLAB_FULL = 2 };
 
 axon_status axon_recall(axon_net* net, const uint32_t* cues, uint32_t B, const axon_recall_args* args,
                         const uint32_t* ref_ball, uint32_t* final_spk, uint32_t* hist, uint32_t* stats,

@@ -201,3 +201,34 @@ def test_tensor_contraction_full_geometry():
     rt = gpu.recall(cues, 45, 10, hist=True, contraction="tensor")
     rp = gpu.recall(cues, 45, 10, hist=True)
     assert np.array_equal(rt["hist"], rp["hist"])
+
+
+@pytest.mark.parametrize("variant", [{}, dict(mode=0, dthr=2), dict(mode=2, dthr=0, boost=9), dict(incols=24)])
+def test_slab_policies_match_oracle(variant):
+    """Which per-neuron drives the batched kernel stores does not change any result: storing
+    only those at or above each trajectory's histogram floor ("floor", the default, and
+    "floor_always", where every drive drop below the floor goes through the recompute)
+    gives the same spikes and counters at every step as storing all ("full"), and the
+    oracle's."""
+    cfg, gpu, cpu, pats = trained_pair(variant, 6, 2, 16)
+    cues = make_cues(pats, cfg.ncol, 37, np.random.default_rng(6))
+    runs = {s: gpu.recall(cues, 20, 5, hist=True, stats=True, slab=s) for s in ("full", "floor", "floor_always")}
+    for s in ("floor", "floor_always"):
+        assert np.array_equal(runs[s]["hist"], runs["full"]["hist"]), s
+        assert np.array_equal(runs[s]["stats"], runs["full"]["stats"]), s
+    f, h, _, _ = oracle_runs(cpu, cues[:5], 20, 5, 0)
+    assert np.array_equal(runs["floor_always"]["hist"][:5], h)
+
+
+@pytest.mark.parametrize("contraction", ["popc", "tensor"])
+def test_slab_policies_full_geometry(contraction):
+    """Config C at full size, 300 cues of 45 steps: the three slab policies agree on every
+    trajectory and step (at the step after the clamp almost every trajectory's threshold
+    falls below its floor, so "floor_always" recomputes many gated columns there)."""
+    cfg, gpu, cpu, pats = trained_pair(dict(ncol=4096, incols=512, target=64, k=24), 12, 2, 64)
+    cues = make_cues(pats, cfg.ncol, 300, np.random.default_rng(3))
+    runs = {s: gpu.recall(cues, 45, 10, hist=True, stats=True, contraction=contraction, slab=s)
+            for s in ("full", "floor", "floor_always")}
+    for s in ("floor", "floor_always"):
+        assert np.array_equal(runs[s]["hist"], runs["full"]["hist"]), s
+        assert np.array_equal(runs[s]["stats"], runs["full"]["stats"]), s
