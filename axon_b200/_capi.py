@@ -123,6 +123,7 @@ def lib() -> C.CDLL:
         L.axon_wdiag.argtypes = [C.c_void_p, U32P, U32P, C.c_uint32, C.c_uint32, U32P]
         L.axon_bstest.argtypes = [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, U32P, U32P, U32P, U32P, U32P,
                                   C.c_uint64]
+        L.axon_kwtatest.argtypes = [C.c_int, U32P, U32P, U32P, C.c_uint32]
         L.axon_set_wait_limit.argtypes = [C.c_void_p, C.c_uint64]
         L.axon_clone.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
         L.axon_profile_present.argtypes = [C.c_void_p, U32P, C.c_uint32, C.c_uint32, C.c_int, C.c_uint32,

@@ -179,8 +179,8 @@ __device__ __forceinline__ void count_drive(uint32_t* h, uint32_t drv) {
 // phase 1's.
 static __device__ __noinline__ uint32_t recall_theta(const uint32_t* sD, const uint32_t* sH, uint32_t* sCand,
                                                      uint32_t* sCtl, uint32_t incols, uint32_t ncol, uint32_t need,
-                                                     uint32_t topkPar) {
-  return hist_theta<-1>(sD, sH, sCand, sCtl, incols, ncol, need, topkPar);
+                                                     uint32_t topkPar, WarpGrp g) {
+  return hist_theta<-1>(sD, sH, sCand, sCtl, incols, ncol, need, topkPar, g);
 }
 
 // The per-neuron drives of column cc for one trajectory, recomputed from that trajectory's
@@ -243,15 +243,6 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   uint32_t* sMisc = sPC + 2 * 68;  // [16]: grid barrier flag, first item, -, -, gated count, -, unit counters [2], next items [2]
   uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
   uint32_t* sFloor = sMisc + 20;  // [B] each trajectory's histogram floor for this step
-  // phase-2 views reuse the tile buffers; a second drive buffer follows them when it fits
-  uint32_t* sSpk = sTile + ncol;
-  uint32_t* sList = sTile + 2 * ncol;
-  uint32_t* sRed = sTile + 3 * ncol;  // 192 words and
-  uint32_t* sHist = sRed + 192;       // 256 words of the sorting threshold select
-  uint32_t* sCtl = sHist + 256;       // 64 words: histogram threshold-select control
-  // the trajectory's drive histogram (and, with two buffers, the next one's drives and
-  // histogram) follow
-  uint32_t* sH0 = sCtl + 64;
 
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
   const uint32_t nitems = (ncol + kRecallCpi - 1) / kRecallCpi;
@@ -562,78 +553,96 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     if (!grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;
 
     // ---------------- phase 2: threshold, gated k-of-32 ballots, next spike vectors and lists
-    // The column drives and the drive histogram of the CTA's trajectories arrive by
-    // asynchronous copies; with two buffers the next trajectory's copies are in flight while
-    // the current one is processed.
-    const bool dbuf = 4u * ncol + 512u + 2u * kHistWords + 32u * nw <= 2u * kItemWords;
-    uint32_t* const sD1 = sH0 + kHistWords;
+    // The CTA works as NG groups of whole warps, each on trajectories of its own, so that their
+    // latency chains (drive copies, threshold select, per-neuron drive loads, ballots, list
+    // appends) overlap: two groups when both groups' buffers fit in the tile region, else one.
+    // A group's buffers: the trajectory's drives, its spike vector and the gated (or candidate)
+    // columns (ncol words each), the select scratch (512), the drive histogram and each warp's
+    // recompute sums. With a second drive buffer (after the first in the tile region with one
+    // group, in the counter region with two) the next trajectory's drives and histogram are in
+    // flight while the current one runs.
+    const uint32_t gWords = 3u * ncol + 512u + kHistWords;
+    const uint32_t NG = (nw % 2u == 0u && 2u * gWords + 32u * nw <= 2u * kItemWords) ? 2u : 1u;
+    const uint32_t gnw = nw / NG, gi = warp / gnw, gw = warp - gi * gnw;
+    const WarpGrp grp{tid - gi * gnw * 32u, gnw * 32u, 1u + gi};
+    uint32_t* const sD0 = sTile + gi * (gWords + 32u * gnw);
+    uint32_t* const sSpk = sD0 + ncol;
+    uint32_t* const sList = sD0 + 2u * ncol;
+    uint32_t* const sRed = sD0 + 3u * ncol;  // 192 words and
+    uint32_t* const sHist = sRed + 192u;      // 256 words of the sorting threshold select
+    uint32_t* const sCtl = sHist + 256u;      // 64 words: select control, gated count
+    uint32_t* const sH0 = sCtl + 64u;         // the drive histogram
+    uint32_t* const sScr = sH0 + kHistWords + 32u * gw;  // this warp's drive recompute sums
+    const bool dbuf = NG == 1u ? gWords + 32u * nw + ncol + kHistWords <= 2u * kItemWords
+                               : NG * (ncol + kHistWords) <= (c.dacc ? 2u : 1u) * accWords;
+    uint32_t* const sD1 = NG == 1u ? sD0 + gWords + 32u * nw : sAcc + gi * (ncol + kHistWords);
     uint32_t* const sH1 = sD1 + ncol;
-    uint32_t* const sScr = (dbuf ? sH1 : sH0) + kHistWords + 32u * warp;  // [nw][32] drive recompute sums
     const uint32_t* hStep = d.thHist + (size_t)(t % 3u) * B * kHistWords;
     auto load_drv = [&](uint32_t b, uint32_t slot) {
       const uint4* src = reinterpret_cast<const uint4*>(d.drv + (size_t)b * ncol);
-      uint4* dst = reinterpret_cast<uint4*>(slot ? sD1 : sTile);
-      for (uint32_t i = tid; i < ncol / 4u; i += blockDim.x) cp_async16(dst + i, src + i);
+      uint4* dst = reinterpret_cast<uint4*>(slot ? sD1 : sD0);
+      for (uint32_t i = grp.t; i < ncol / 4u; i += grp.nt) cp_async16(dst + i, src + i);
       const uint4* hs = reinterpret_cast<const uint4*>(hStep + (size_t)b * kHistWords);
       uint4* hd = reinterpret_cast<uint4*>(slot ? sH1 : sH0);
-      for (uint32_t i = tid; i < kHistWords / 4u; i += blockDim.x) cp_async16(hd + i, hs + i);
+      for (uint32_t i = grp.t; i < kHistWords / 4u; i += grp.nt) cp_async16(hd + i, hs + i);
     };
-    // Tasks: trajectory blockIdx + k * grid for the full rounds k < F. The R < grid
-    // trajectories of the last round are split, when each can have at least two CTAs, into
-    // P = grid / R parts, each on a range of whole groups (8 columns): every part selects
-    // the same threshold, then gates, ballots, writes and lists only its own columns, so the
-    // last round costs about one threshold select instead of a whole trajectory.
-    const uint32_t G = gridDim.x, F = B / G, R = B - F * G;
-    const uint32_t P = R ? G / R : 0u;
+    // Tasks of worker wid (W = NG per CTA): trajectory wid + k * W for the full rounds k < F.
+    // The R < W trajectories of the last round are split, when each can have at least two
+    // workers, into P = W / R parts, each on a range of whole groups (8 columns): every part
+    // selects the same threshold, then gates, ballots, writes and lists only its own columns,
+    // so the last round costs about one threshold select instead of a whole trajectory.
+    const uint32_t W = gridDim.x * NG, wid = blockIdx.x * NG + gi;
+    const uint32_t F = B / W, R = B - F * W;
+    const uint32_t P = R ? W / R : 0u;
     const bool split = P >= 2u;
-    const uint32_t ntask = F + (R != 0u && blockIdx.x < (split ? R * P : R) ? 1u : 0u);
-    auto task_b = [&](uint32_t k) { return k < F ? blockIdx.x + k * G : F * G + (split ? blockIdx.x / P : blockIdx.x); };
+    const uint32_t ntask = F + (R != 0u && wid < (split ? R * P : R) ? 1u : 0u);
+    auto task_b = [&](uint32_t k) { return k < F ? wid + k * W : F * W + (split ? wid / P : wid); };
     if (ntask) load_drv(task_b(0), 0);
     cp_async_commit();
     for (uint32_t k = 0; k < ntask; ++k) {
       const uint32_t b = task_b(k);
       const bool part = split && k == F;
-      const uint32_t pi = part ? blockIdx.x % P : 0u, np = part ? P : 1u;
+      const uint32_t pi = part ? wid % P : 0u, np = part ? P : 1u;
       const uint32_t gLo = pi * ngrp / np, gHi = (pi + 1u) * ngrp / np, cLo = 8u * gLo, cHi = 8u * gHi;
       const uint32_t slot = dbuf ? (k & 1u) : 0u;
-      uint32_t* sD = slot ? sD1 : sTile;
+      uint32_t* sD = slot ? sD1 : sD0;
       const uint32_t* sH = slot ? sH1 : sH0;
       const bool hasNext = k + 1u < ntask;
       if (dbuf && hasNext) load_drv(task_b(k + 1u), slot ^ 1u);
       cp_async_commit();
       if (dbuf) cp_async_wait<1>();  // all but the copies just issued: this trajectory's
       else cp_async_wait<0>();
-      if (tid == 0) { sMisc[4] = 0u; sCtl[0] = 0u; }
-      __syncthreads();  // every thread's copies have landed
-      if (warp == 0) {  // drives the histogram holds
+      if (grp.t == 0) { sCtl[9] = 0u; sCtl[0] = 0u; }
+      grp.sync();  // every thread's copies have landed
+      if (gw == 0) {  // drives the histogram holds
         uint32_t n = 0;
         for (uint32_t i = lane; i < kThetaBins; i += 32u) n += sH[i];
         n = __reduce_add_sync(kFull, n);
         if (lane == 0) sCtl[8] = n;
       }
-      __syncthreads();
+      grp.sync();
       // gated columns whose drive is below reFloor have no slab entry (a fallback select)
       const uint32_t reFloor = fast && !storeAll && sCtl[8] < c.targetCols ? sFloor[b] : 0u;
       const uint32_t theta = sCtl[8] >= c.targetCols
-                                 ? recall_theta(sD, sH, sList, sCtl, incols, ncol, c.targetCols, c.topkPar)
+                                 ? recall_theta(sD, sH, sList, sCtl, incols, ncol, c.targetCols, c.topkPar, grp)
                                  : block_theta(sD, incols, ncol, c.targetCols, c.topkPar, sHist, sRed,
-                                               __ldcg(d.thPrev + b));
+                                               __ldcg(d.thPrev + b), grp);
       // this trajectory's histogram of step t+1 mod 3, last read two steps ago, is cleared
       // for phase 1 of the next step
       if (pi == 0u) {
         uint4* hz = reinterpret_cast<uint4*>(d.thHist + ((size_t)((t + 1u) % 3u) * B + b) * kHistWords);
-        for (uint32_t i = tid; i < kHistWords / 4u; i += blockDim.x) __stcg(hz + i, make_uint4(0u, 0u, 0u, 0u));
+        for (uint32_t i = grp.t; i < kHistWords / 4u; i += grp.nt) __stcg(hz + i, make_uint4(0u, 0u, 0u, 0u));
       }
       const uint32_t gate = max(theta, 1u);
       const uint32_t* stimb = d.stims + (size_t)b * ncol;
-      for (uint32_t cc = cLo + tid; cc < cHi; cc += blockDim.x) {
+      for (uint32_t cc = cLo + grp.t; cc < cHi; cc += grp.nt) {
         uint32_t v = 0u;
         if (clamp && cc < incols) v = __ldg(stimb + cc);
-        else if (sD[cc] >= gate) sList[atomicAdd(sMisc + 4, 1u)] = cc;
+        else if (sD[cc] >= gate) sList[atomicAdd(sCtl + 9, 1u)] = cc;
         sSpk[cc] = v;
       }
-      __syncthreads();
-      const uint32_t npend = sMisc[4];
+      grp.sync();
+      const uint32_t npend = sCtl[9];
       // k-of-32 of one gated column from its per-neuron drive a (one per lane)
       auto emit_col = [&](uint32_t cc, uint32_t a) {
         uint32_t vk, vk1;
@@ -657,7 +666,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       if (reFloor != 0u) {
         sScr[lane] = 0u;
         __syncwarp();
-        for (uint32_t e = warp; e < npend; e += nw) {
+        for (uint32_t e = gw; e < npend; e += gnw) {
           const uint32_t cc = sList[e];
           if (sD[cc] < reFloor)
             emit_col(cc, recompute_drive<LIN>(d.W3R, d.conn, spkIn + (size_t)b * ncol, cc, dthr, bst, lane, sScr));
@@ -665,12 +674,12 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       }
       // the others from the slab, a warp's gated columns kPend at a time: their per-neuron
       // drives load together
-      constexpr uint32_t kPend = 4;
-      for (uint32_t e0 = warp; e0 < npend; e0 += kPend * nw) {
+      constexpr uint32_t kPend = 8;
+      for (uint32_t e0 = gw; e0 < npend; e0 += kPend * gnw) {
         uint32_t av[kPend];
 #pragma unroll
         for (uint32_t u = 0; u < kPend; ++u) {
-          const uint32_t e = e0 + u * nw;
+          const uint32_t e = e0 + u * gnw;
           av[u] = 0u;
           if (e < npend && sD[sList[e]] >= reFloor) {
             const size_t o = ((size_t)b * ncol + sList[e]) * 32u + lane;
@@ -680,22 +689,22 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         }
 #pragma unroll
         for (uint32_t u = 0; u < kPend; ++u) {
-          const uint32_t e = e0 + u * nw;
+          const uint32_t e = e0 + u * gnw;
           if (e >= npend) break;  // warp-uniform
           const uint32_t cc = sList[e];
           if (sD[cc] >= reFloor) emit_col(cc, av[u]);
         }
       }
-      __syncthreads();
+      grp.sync();
       uint32_t* outb = spkOut + (size_t)b * ncol;
-      for (uint32_t i = cLo / 4u + tid; i < cHi / 4u; i += blockDim.x) {
+      for (uint32_t i = cLo / 4u + grp.t; i < cHi / 4u; i += grp.nt) {
         const uint4 v = reinterpret_cast<const uint4*>(sSpk)[i];
         __stcg(reinterpret_cast<uint4*>(outb) + i, v);
         if (d.hist) reinterpret_cast<uint4*>(d.hist + ((size_t)b * c.T + t) * ncol)[i] = v;
         if (d.finalOut && t + 1u == c.T) reinterpret_cast<uint4*>(d.finalOut + (size_t)b * ncol)[i] = v;
       }
       if (t + 1u < c.T) {  // group lists for the next step
-        for (uint32_t g = gLo + tid; g < gHi; g += blockDim.x) {
+        for (uint32_t g = gLo + grp.t; g < gHi; g += grp.nt) {
           const uint4 p = reinterpret_cast<const uint4*>(sSpk)[2 * g], q = reinterpret_cast<const uint4*>(sSpk)[2 * g + 1];
           const uint32_t w[8] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w};
           uint32_t nz = 0, S0 = 0u, S1 = 0u, S2 = 0u, k = 0, w0 = 0;
@@ -717,14 +726,19 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
           }
         }
       }
-      if (tid == 0 && pi == 0u) {
+      if (grp.t == 0 && pi == 0u) {
         __stcg(d.thPrev + b, theta);
         if (d.theta && t + 1u == c.T) d.theta[b] = theta;
       }
-      __syncthreads();
+      grp.sync();
       if (!dbuf && hasNext) load_drv(task_b(k + 1u), 0);  // committed at the next task's start
     }
     cp_async_wait<0>();
+    // second drive buffers in the counter region: zero again before the next phase 1
+    if (NG == 2u && dbuf) {
+      __syncthreads();
+      for (uint32_t i = tid; i < NG * (ncol + kHistWords); i += blockDim.x) sAcc[i] = 0u;
+    }
     if (t + 1u < c.T && !grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;
   }
 }

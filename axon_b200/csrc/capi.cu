@@ -137,6 +137,21 @@ axon_status axon_bstest(int device, uint32_t op, uint32_t lo, uint32_t hi, uint3
   return AXON_OK;
 }
 
+axon_status axon_kwtatest(int device, const uint32_t* v, const uint32_t* k, uint32_t* out, uint32_t n) {
+  if (!v || !k || !out || n == 0) return fail(AXON_EINVAL, "bad argument");
+  CK(cudaSetDevice(device));
+  uint32_t* d = nullptr;
+  CK(cudaMalloc(&d, (size_t)n * 36u * sizeof(uint32_t)));
+  cudaError_t e = cudaMemcpy(d, v, (size_t)n * 32u * 4u, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + (size_t)n * 32u, k, (size_t)n * 4u, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = launch_kwtatest(d, d + (size_t)n * 32u, d + (size_t)n * 33u, n, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(out, d + (size_t)n * 33u, (size_t)n * 12u, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "axon_kwtatest");
+  return AXON_OK;
+}
+
 axon_status axon_clone(const axon_net* src, axon_net** out) {
   if (!src || !out) return fail(AXON_EINVAL, "null argument");
   *out = nullptr;

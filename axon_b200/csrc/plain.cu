@@ -621,6 +621,20 @@ __global__ void k_bstest(uint32_t* A0, uint32_t* A1, uint32_t* A2, uint32_t* A3,
   A0[g] = a0; A1[g] = a1; A2[g] = a2; A3[g] = a3;
 }
 
+// The kernels' k-of-32 (warp_kwta, src/axon.mm:134-144) on n columns of 32 values, one warp
+// per column: out[3i..3i+2] = winners ballot, vk, vk1.
+__global__ void k_kwtatest(const uint32_t* v, const uint32_t* k, uint32_t* out, uint32_t n) {
+  const uint32_t lane = threadIdx.x & 31u, col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (col >= n) return;  // whole warps
+  uint32_t vk, vk1;
+  const uint32_t ball = warp_kwta(v[(size_t)col * 32u + lane], lane, k[col], vk, vk1);
+  if (lane == 0) {
+    out[3u * col] = ball;
+    out[3u * col + 1u] = vk;
+    out[3u * col + 2u] = vk1;
+  }
+}
+
 cudaError_t launch_wstat(const NetDev& d, uint32_t ncol, uint32_t* out, cudaStream_t st) {
   const uint64_t nU4 = (uint64_t)ncol * kNslot * kTileU4;
   k_wstat<<<148 * 8, 256, 0, st>>>(d.W3, nU4, out);
@@ -646,6 +660,10 @@ cudaError_t launch_wdiag(const NetDev& d, uint32_t ncol, const uint32_t* memb, c
 cudaError_t launch_bstest(uint32_t* a0, uint32_t* a1, uint32_t* a2, uint32_t* a3, const uint32_t* m, uint32_t op,
                           uint32_t lo, uint32_t hi, uint64_t n, cudaStream_t st) {
   k_bstest<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a0, a1, a2, a3, m, op, lo, hi, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_kwtatest(const uint32_t* v, const uint32_t* k, uint32_t* out, uint32_t n, cudaStream_t st) {
+  k_kwtatest<<<(n + 7u) / 8u, 256, 0, st>>>(v, k, out, n);
   return cudaGetLastError();
 }
 

@@ -81,5 +81,6 @@ cudaError_t launch_wdiag(const NetDev& d, uint32_t ncol, const uint32_t* memb, c
                          uint32_t inBr, uint32_t sel, uint32_t* hist, cudaStream_t st);
 cudaError_t launch_bstest(uint32_t* a0, uint32_t* a1, uint32_t* a2, uint32_t* a3, const uint32_t* m, uint32_t op,
                           uint32_t lo, uint32_t hi, uint64_t n, cudaStream_t st);
+cudaError_t launch_kwtatest(const uint32_t* v, const uint32_t* k, uint32_t* out, uint32_t n, cudaStream_t st);
 
 }  // namespace axon

@@ -6,6 +6,23 @@
 
 namespace axon {
 
+// The threads that run a threshold select together: the whole block (BlockGrp, synchronised
+// by the block barrier), or a set of whole warps with a named barrier of its own (WarpGrp), so
+// that several groups of one block can each select for a trajectory of their own at once.
+struct BlockGrp {
+  __device__ __forceinline__ uint32_t tid() const { return threadIdx.x; }
+  __device__ __forceinline__ uint32_t n() const { return blockDim.x; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+struct WarpGrp {
+  uint32_t t;    // thread index within the group
+  uint32_t nt;   // threads in the group, a multiple of 32
+  uint32_t bar;  // named barrier id, 1..15, used by this group alone
+  __device__ __forceinline__ uint32_t tid() const { return t; }
+  __device__ __forceinline__ uint32_t n() const { return nt; }
+  __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(nt) : "memory"); }
+};
+
 // Exact selection of the column threshold over recurrent columns [incols, ncol),
 // src/axon.mm:301-352 (k_topk_par, default) and :259-292 (k_topk_serial). Both return
 // max(v, 1) where v is the need-th largest drive among drives below 2^24 when at least
@@ -21,16 +38,17 @@ namespace axon {
 // threshold 1. `hint` is a guess of the answer (the previous step's threshold; 0 for
 // none): when at least `need` drives reach it (or half of it), only those drives take part,
 // which keeps the histogram small. The result does not depend on the hint.
-// Every thread of the block calls it; sHist holds 256 words, sRed 96.
+// Every thread of the group g calls it; sHist holds 256 words, sRed 192.
+template <class G = BlockGrp>
 static __device__ __noinline__ uint32_t block_theta(const uint32_t* sD, uint32_t incols, uint32_t ncol, uint32_t need,
                                                     uint32_t topkPar, uint32_t* sHist, uint32_t* sRed,
-                                                    uint32_t hint) {
-  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
+                                                    uint32_t hint, G g = G{}) {
+  const uint32_t tid = g.tid(), lane = tid & 31u, warp = tid >> 5, nw = g.n() >> 5;
   const uint32_t h1 = max(hint, 1u), h2 = max(hint >> 1, 1u);
   // largest candidate, number of candidates, of positive candidates, and of candidates
   // reaching the hint and half the hint
   uint32_t mx = 0, cnt = 0, pos = 0, n1 = 0, n2 = 0;
-  for (uint32_t c = incols + tid; c < ncol; c += blockDim.x) {
+  for (uint32_t c = incols + tid; c < ncol; c += g.n()) {
     const uint32_t d = sD[c];
     if (d < (1u << 24)) { mx = max(mx, d); ++cnt; pos += d != 0u; n1 += d >= h1; n2 += d >= h2; }
   }
@@ -40,8 +58,8 @@ static __device__ __noinline__ uint32_t block_theta(const uint32_t* sD, uint32_t
   n1 = __reduce_add_sync(kFull, n1);
   n2 = __reduce_add_sync(kFull, n2);
   if (lane == 0) { sRed[warp] = mx; sRed[32 + warp] = cnt; sRed[64 + warp] = pos; sRed[128 + warp] = n1; sRed[160 + warp] = n2; }
-  for (uint32_t i = tid; i < 256u; i += blockDim.x) sHist[i] = 0u;
-  __syncthreads();
+  for (uint32_t i = tid; i < 256u; i += g.n()) sHist[i] = 0u;
+  g.sync();
   uint32_t M, count, npos, lo;
   {
     const bool v = lane < nw;
@@ -52,8 +70,8 @@ static __device__ __noinline__ uint32_t block_theta(const uint32_t* sD, uint32_t
     const uint32_t c2 = __reduce_add_sync(kFull, v ? sRed[160 + lane] : 0u);
     lo = c1 >= need ? h1 : (c2 >= need ? h2 : 1u);  // every drive below lo ranks below the answer
   }
-  if (need == 0u) { __syncthreads(); return topkPar ? 1u : 0xFFFFFFu; }
-  if (count < need || npos < need) { __syncthreads(); return 1u; }
+  if (need == 0u) { g.sync(); return topkPar ? 1u : 0xFFFFFFu; }
+  if (count < need || npos < need) { g.sync(); return 1u; }
 
   // select the need-th largest x = d - lo over the candidates d in [lo, 2^24)
   const uint32_t nb = 32u - __clz(max(M - lo, 1u));
@@ -63,14 +81,14 @@ static __device__ __noinline__ uint32_t block_theta(const uint32_t* sD, uint32_t
     const uint32_t width = (hiShift >= 32u ? nb : hiShift) - shift;  // 1..8
     const uint32_t dmask = (1u << width) - 1u;
     // bins were cleared before the previous sync
-    for (uint32_t c = incols + tid; c < ncol; c += blockDim.x) {
+    for (uint32_t c = incols + tid; c < ncol; c += g.n()) {
       const uint32_t d = sD[c];
       if (d < lo || d >= (1u << 24)) continue;
       const uint32_t x = d - lo;
       if (hiShift < 32u && (x >> hiShift) != (prefix >> hiShift)) continue;
       atomicAdd(&sHist[(x >> shift) & dmask], 1u);
     }
-    __syncthreads();
+    g.sync();
     if (warp == 0) {  // bin where the count from the top reaches rem; then clear the bins
       uint32_t h[8], ls = 0;
 #pragma unroll
@@ -97,14 +115,14 @@ static __device__ __noinline__ uint32_t block_theta(const uint32_t* sD, uint32_t
 #pragma unroll
       for (int i = 0; i < 8; ++i) sHist[lane * 8 + i] = 0u;
     }
-    __syncthreads();
+    g.sync();
     prefix |= sRed[94] << shift;
     rem -= sRed[95];
     if (shift == 0u) break;
     hiShift = shift;
     shift = shift >= 8u ? shift - 8u : 0u;
   }
-  __syncthreads();
+  g.sync();
   return max(prefix + lo, 1u);
 }
 
@@ -129,17 +147,17 @@ __device__ __forceinline__ uint32_t theta_bin_lo(uint32_t k) { return k < 64u ? 
 // or smallest drive when it ranks first or last in its bin; otherwise the block collects
 // the bin's drives (usually a few) into sCand and warp 0 resolves the rank bit by bit, most
 // significant first. sCtl[0] is the candidate counter and must be zero on entry;
-// sCtl[2..5] is scratch. Every thread of the block calls it. The histogram must be in shared
+// sCtl[2..5] is scratch. Every thread of the group g calls it. The histogram must be in shared
 // memory on entry; the drives are read only after the scan, so with kDrivesGroup >= 0 they may
 // still be arriving by asynchronous copy: each thread then waits until at most kDrivesGroup of
-// its copy groups are pending before the block barrier that precedes the first read.
-template <int kDrivesGroup = -1>
+// its copy groups are pending before the group barrier that precedes the first read.
+template <int kDrivesGroup = -1, class G = BlockGrp>
 static __device__ __forceinline__ uint32_t hist_theta(const uint32_t* sD, const uint32_t* sH, uint32_t* sCand,
                                                    uint32_t* sCtl, uint32_t incols, uint32_t ncol, uint32_t need,
-                                                   uint32_t topkPar) {
+                                                   uint32_t topkPar, G g = G{}) {
   constexpr uint32_t kPer = 20;  // bins per lane (640 / 32)
   constexpr uint32_t kThetaBinCount = 32u * kPer;
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t lane = g.tid() & 31u, warp = g.tid() >> 5;
   if (warp == 0u) {
     uint32_t h[kPer], ls = 0;
     const uint4* h4 = reinterpret_cast<const uint4*>(sH + lane * kPer);
@@ -185,16 +203,16 @@ static __device__ __forceinline__ uint32_t hist_theta(const uint32_t* sD, const 
     if (lane == 0u) { sCtl[2] = res; sCtl[3] = b; sCtl[4] = need - above; sCtl[5] = inBin; }
   }
   if constexpr (kDrivesGroup >= 0) cp_async_wait<kDrivesGroup>();
-  __syncthreads();
+  g.sync();
   const uint32_t res = sCtl[2];
   if (res != 0u) return res;
   const uint32_t b = sCtl[3];
   const uint32_t bits = (b >> 5) - 1u, lo = (32u | (b & 31u)) << bits;
-  for (uint32_t c = incols + threadIdx.x; c < ncol; c += blockDim.x) {
+  for (uint32_t c = incols + g.tid(); c < ncol; c += g.n()) {
     const uint32_t d = sD[c];
     if (d < (1u << 24) && theta_key(d) == b) sCand[atomicAdd(sCtl, 1u)] = d - lo;
   }
-  __syncthreads();
+  g.sync();
   if (warp == 0u) {
     uint32_t rem = sCtl[4];  // rank of the answer among the drives of bin b, from the top
     const uint32_t inBin = sCtl[5];
@@ -219,7 +237,7 @@ static __device__ __forceinline__ uint32_t hist_theta(const uint32_t* sD, const 
     }
     if (lane == 0u) sCtl[2] = lo + prefix;
   }
-  __syncthreads();
+  g.sync();
   return sCtl[2];
 }
 

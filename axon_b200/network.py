@@ -330,6 +330,17 @@ def noisy_cue_seed(q: int, pct: int, draw: int) -> int:
     return int(A.lib().axon_noisy_cue_seed(q, pct, draw))
 
 
+def kwtatest(values: np.ndarray, ks: np.ndarray, device: int = 0) -> np.ndarray:
+    """Runs the kernels' k-of-32 on (n, 32) values with one k per row: (n, 3) = winners
+    ballot, vk, vk1."""
+    v = np.ascontiguousarray(values, dtype=np.uint32)
+    k = np.ascontiguousarray(ks, dtype=np.uint32)
+    assert v.shape == (k.size, 32)
+    out = np.zeros((k.size, 3), dtype=np.uint32)
+    A.check(A.lib().axon_kwtatest(device, A.u32(v), A.u32(k), A.u32(out), k.size))
+    return out
+
+
 def bstest(op: int, lo: int, hi: int, planes: list[np.ndarray], mask: np.ndarray, device: int = 0) -> None:
     """Runs the bit-serial inc/dec/clip kernel in place on four planes (k_bstest)."""
     ps = [np.ascontiguousarray(p, dtype=np.uint32) for p in planes]

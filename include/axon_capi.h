@@ -129,6 +129,10 @@ axon_status axon_wdiag(axon_net* net, const uint32_t* memb, const uint32_t* asm_
  * words each (n a multiple of 4); op 0 inc, 1 dec, 2 clip [lo,hi]; planes updated. */
 axon_status axon_bstest(int device, uint32_t op, uint32_t lo, uint32_t hi, uint32_t* a0,
                         uint32_t* a1, uint32_t* a2, uint32_t* a3, const uint32_t* m, uint64_t n);
+/* k-of-32 known-answer hook: the kernels' exact k-WTA ranking (kwta_ballot_margin,
+ * src/axon.mm:134-144) on n columns: v holds 32 values per column, k one k per column;
+ * out receives per column the winners ballot, vk and vk1 (3 words). */
+axon_status axon_kwtatest(int device, const uint32_t* v, const uint32_t* k, uint32_t* out, uint32_t n);
 
 /* Stimulus patterns: `nstim` rows of `stimcols` input-column indices, drawn as
  * src/axon.mm:793-799 does (mt19937(7 + seed*104729), libc++ shuffle of 0..incols-1). */

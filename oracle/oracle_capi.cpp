@@ -142,6 +142,12 @@ void oracle_bstest(uint32_t op, uint32_t lo, uint32_t hi, uint32_t* a0, uint32_t
   }
 }
 
+// k-of-32 ranking on n columns of 32 values (kwta_ballot_margin, src/axon.mm:134-144):
+// out[3i..3i+2] = winners ballot, vk, vk1
+void oracle_kwtatest(const uint32_t* v, const uint32_t* k, uint32_t* out, uint32_t n) {
+  for (uint32_t i = 0; i < n; ++i) out[3u * i] = oracle::kwta_ballot_margin(v + 32ull * i, k[i], out[3u * i + 1], out[3u * i + 2]);
+}
+
 // stimulus patterns of src/axon.mm:793-799: nstim x stimcols column indices
 void oracle_stimuli(uint32_t seed, uint32_t nstim, uint32_t incols, uint32_t stimcols, uint32_t* out) {
   std::mt19937 rng(7u + seed * 104729u);

@@ -71,6 +71,7 @@ def load():
         L.oracle_untouched.argtypes = [C.c_void_p, U32P]
         L.oracle_wdiag.argtypes = [C.c_void_p, U32P, U32P, C.c_uint32, C.c_uint32, U32P]
         L.oracle_bstest.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, U32P, U32P, U32P, U32P, U32P, C.c_uint64]
+        L.oracle_kwtatest.argtypes = [U32P, U32P, U32P, C.c_uint32]
         L.oracle_stimuli.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, U32P]
         L.oracle_load_stim.argtypes = [U32P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, U32P]
         L.oracle_uniform_int.argtypes = [C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(C.c_uint64)]
@@ -191,6 +192,15 @@ def bstest(op, lo, hi, planes, mask):
     m = np.ascontiguousarray(mask, dtype=np.uint32)
     load().oracle_bstest(op, lo, hi, *(u32(p) for p in ps), u32(m), m.size)
     return ps
+
+
+def kwtatest(values, ks):
+    """The oracle's k-of-32 ranking on (n, 32) values: (n, 3) = ballot, vk, vk1."""
+    v = np.ascontiguousarray(values, dtype=np.uint32)
+    k = np.ascontiguousarray(ks, dtype=np.uint32)
+    out = np.zeros((k.size, 3), dtype=np.uint32)
+    load().oracle_kwtatest(u32(v), u32(k), u32(out), k.size)
+    return out
 
 
 def run_cli(args: list[str], threads: int | None = None, timeout: float = 3600) -> str:

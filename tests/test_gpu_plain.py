@@ -232,3 +232,13 @@ def test_dense_activity_overflows_tile_pool(target, inbr):
     compare(gpu, cpu, BUFS_EACH_PRESENT + ["HIST"], T=8, where="dense readout")
     gpu.close()
     cpu.close()
+
+
+def test_kwta_kat_gpu():
+    """The kernels' k-of-32 equals the oracle's on ties, spread and large values (the rank-
+    count form below 2^27, the radix select above) for every k from 0 to 33."""
+    import axon_b200 as ax
+    from test_oracle_pins import kwta_cases
+
+    v, ks = kwta_cases()
+    assert np.array_equal(ax.kwtatest(v, ks), O.kwtatest(v, ks))

@@ -134,3 +134,37 @@ def test_table2_fixture_matches_paper():
         for f in ("sustained_mean", "sustained_sd", "margin_mean", "margin_sd", "within_mean", "within_sd"):
             assert got[f] == row[f], (row["stim"], f, got[f], row[f])
     assert fx["summary"]["12"]["sustained_mean"] == t2["stim12_sustained_mean"]
+
+
+def kwta_cases(seed=11):
+    """Columns of 32 values for the k-of-32 known-answer tests: heavy ties (values 0..3),
+    spread values, values at and above 2^27 and near 2^32, all-equal and all-zero columns,
+    with every k from 0 to 33."""
+    rng = np.random.default_rng(seed)
+    cols, ks = [], []
+    for k in range(34):
+        for hi in (1, 4, 40, 1 << 16, 1 << 27, 1 << 32):
+            for _ in range(6):
+                cols.append(rng.integers(0, hi, 32, dtype=np.uint64).astype(np.uint32))
+                ks.append(k)
+        cols.append(np.full(32, 7, dtype=np.uint32)); ks.append(k)
+        cols.append(np.zeros(32, dtype=np.uint32)); ks.append(k)
+        big = rng.integers((1 << 27) - 3, (1 << 27) + 3, 32, dtype=np.uint64).astype(np.uint32)
+        cols.append(big); ks.append(k)
+    return np.stack(cols), np.array(ks, dtype=np.uint32)
+
+
+def test_kwta_oracle_matches_rank_definition():
+    """The oracle's k-of-32 (src/axon.mm:134-144) against the rank definition computed here:
+    rank_i = #{j : v_j > v_i or (v_j == v_i and j < i)}, winners rank < k, vk and vk1 the
+    values ranked k-1 and k."""
+    v, ks = kwta_cases()
+    got = O.kwtatest(v, ks)
+    for i in range(len(ks)):
+        x = v[i].astype(np.int64)
+        rank = np.array([np.sum((x > x[a]) | ((x == x[a]) & (np.arange(32) < a))) for a in range(32)])
+        k = int(ks[i])
+        ball = sum(1 << a for a in range(32) if rank[a] < k)
+        vk = int(x[rank == k - 1][0]) if k >= 1 and k <= 32 else 0
+        vk1 = int(x[rank == k][0]) if k <= 31 else 0
+        assert (int(got[i, 0]), int(got[i, 1]), int(got[i, 2])) == (ball, vk, vk1), (i, k)
