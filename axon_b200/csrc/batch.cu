@@ -474,43 +474,45 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       if (tid == 0) sMisc[6 + bcur] = 0u;  // every warp has claimed its units of this item
       // per-neuron and column drives of the item's columns for every trajectory
       if (fast) {
-        // the packed counters already are the u16 drive slab: four lanes per (column,
-        // trajectory), each storing 4 of its 16 words as one 16-byte vector
-        // (column, trajectory) pairs in column-major order: the trajectory index steps by
-        // 8 x warps, with no division
-        const uint32_t q = lane & 3u, grp = lane >> 2;
-        const uint32_t gmask = 0xFu << (grp * 4u);
-        const uint32_t ncl = min(kRecallCpi, ncol - c0);
-        uint32_t colL = 0, b = warp * 8u + grp;
-        while (b >= B && colL < ncl) { b -= B; ++colL; }
-        while (colL < ncl) {  // uniform over the four lanes of a pair
-          const uint32_t col = c0 + colL;
-          uint32_t* src = acc_row<PACK>(accB, colL * B + b) + q * 4u;
-          uint4 w = make_uint4(src[0], src[1], src[2], src[3]);
-          src[0] = src[1] = src[2] = src[3] = 0u;
+        // the packed counters already are the u16 drive slab. One (column, trajectory) pair
+        // per thread, pairs in column-major order: its 16 counter words are read and cleared
+        // with scalar shared accesses (rows are 17 words apart, so 32 consecutive rows fall
+        // on 32 banks), summed in registers and stored as 64 contiguous bytes
+        const uint32_t np = min(kRecallCpi, ncol - c0) * B;
+        for (uint32_t p = tid; p < np; p += blockDim.x) {
+          const uint32_t colL = p / B, b = p - colL * B, col = c0 + colL;
+          uint32_t* src = acc_row<PACK>(accB, p);
+          uint32_t w[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) w[i] = src[i];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) src[i] = 0u;
           if (affStore || affAdd) {  // the afferent cache (halves add without carry: drives stay below 2^16)
-            uint4* ap = reinterpret_cast<uint4*>(d.aff) + ((size_t)b * ncol + col) * 4u + q;
-            if (affStore) {
-              __stcg(ap, w);
-            } else {
-              const uint4 a = __ldcg(ap);
-              w.x += a.x; w.y += a.y; w.z += a.z; w.w += a.w;
+            // laid out [column][quad][trajectory]: consecutive threads touch consecutive quads
+            uint4* ap = reinterpret_cast<uint4*>(d.aff) + (size_t)col * 4u * B + b;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              if (affStore) {
+                __stcg(ap + (size_t)j * B, make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]));
+              } else {
+                const uint4 a = __ldcg(ap + (size_t)j * B);
+                w[4 * j] += a.x; w[4 * j + 1] += a.y; w[4 * j + 2] += a.z; w[4 * j + 3] += a.w;
+              }
             }
           }
-          // sum of the 8 per-neuron drives in w: each word is lo + 65536 hi, so lo + hi is
-          // the word minus 65535 hi
-          uint32_t s = (w.x - 65535u * (w.x >> 16)) + (w.y - 65535u * (w.y >> 16)) + (w.z - 65535u * (w.z >> 16)) +
-                       (w.w - 65535u * (w.w >> 16));
-          s += __shfl_xor_sync(gmask, s, 1);
-          s += __shfl_xor_sync(gmask, s, 2);
+          // sum of the 32 per-neuron drives: each word is lo + 65536 hi, so lo + hi is the
+          // word minus 65535 hi
+          uint32_t s = 0u;
+#pragma unroll
+          for (int i = 0; i < 16; ++i) s += w[i] - 65535u * (w[i] >> 16);
           const uint32_t fl = sFloor[b];
-          if (storeAll || s >= fl) reinterpret_cast<uint4*>(d.acc)[((size_t)b * ncol + col) * 4u + q] = w;
-          if (q == 0) {
-            __stcg(d.drv + (size_t)b * ncol + col, s);
-            if (col >= incols && s >= fl) count_drive(d.thHist + ((size_t)(t % 3u) * B + b) * kHistWords, s);
+          if (storeAll || s >= fl) {
+            uint4* dst = reinterpret_cast<uint4*>(d.acc) + ((size_t)b * ncol + col) * 4u;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) dst[j] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
           }
-          b += nw * 8u;
-          while (b >= B && colL < ncl) { b -= B; ++colL; }
+          __stcg(d.drv + (size_t)b * ncol + col, s);
+          if (col >= incols && s >= fl) count_drive(d.thHist + ((size_t)(t % 3u) * B + b) * kHistWords, s);
         }
       } else {
         for (uint32_t pp = warp; pp < kRecallCpi * B; pp += nw) {

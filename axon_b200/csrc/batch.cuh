@@ -33,7 +33,7 @@ struct RecallDev {
   uint32_t* theta;          // [B] threshold of the last step, or null
   uint32_t* thHist;         // [3][B][3 x 640] drive histograms by step mod 3 (zeroed before launch)
   uint32_t* thPrev;         // [B] each trajectory's latest threshold (zeroed before launch)
-  uint32_t* aff;            // [B][ncol][16] afferent counters of the clamped steps (packed fast path), or null
+  uint32_t* aff;            // [ncol][4][B] x 4 words: afferent counters of the clamped steps (packed fast path), or null
   uint32_t* work;           // [max(T, 64)] phase-1 work counters (zeroed before launch)
   uint32_t* bar;            // grid barrier counter (zeroed before launch)
   uint32_t* err;            // device error word
