@@ -557,17 +557,23 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     // ---------------- phase 2: threshold, gated k-of-32 ballots, next spike vectors and lists
     // The CTA works as NG groups of whole warps, each on trajectories of its own, so that their
     // latency chains (drive copies, threshold select, per-neuron drive loads, ballots, list
-    // appends) overlap: two groups when both groups' buffers fit in the tile region, else one.
-    // A group's buffers: the trajectory's drives, its spike vector and the gated (or candidate)
-    // columns (ncol words each), the select scratch (512), the drive histogram and each warp's
-    // recompute sums. With a second drive buffer (after the first in the tile region with one
-    // group, in the counter region with two) the next trajectory's drives and histogram are in
-    // flight while the current one runs.
+    // appends) overlap: up to three groups, as many as the tile and counter regions (one
+    // contiguous range, both idle in phase 2) hold. A group's buffers: the trajectory's drives,
+    // its spike vector and the gated (or candidate) columns (ncol words each), the select
+    // scratch (512), the drive histogram and each warp's recompute sums. With second drive
+    // buffers after all groups' buffers, the next trajectory's drives and histogram are in
+    // flight while the current one runs. Whatever of the counter region this uses is zeroed
+    // again before phase 1.
     const uint32_t gWords = 3u * ncol + 512u + kHistWords;
-    const uint32_t NG = (nw % 2u == 0u && 2u * gWords + 32u * nw <= 2u * kItemWords) ? 2u : 1u;
-    const uint32_t gnw = nw / NG, gi = warp / gnw, gw = warp - gi * gnw;
-    const WarpGrp grp{tid - gi * gnw * 32u, gnw * 32u, 1u + gi};
-    uint32_t* const sD0 = sTile + gi * (gWords + 32u * gnw);
+    const uint32_t avail = 2u * kItemWords + (c.dacc ? 2u : 1u) * accWords;
+    const uint32_t NG = nw >= 3u && 3u * gWords + 32u * nw <= avail ? 3u : nw >= 2u && 2u * gWords + 32u * nw <= avail ? 2u : 1u;
+    // group gi has warps [w0, w0 + gnw): the first nw % NG groups one warp more
+    const uint32_t gq = nw / NG, gx = nw % NG;
+    const uint32_t gi = warp < gx * (gq + 1u) ? warp / (gq + 1u) : gx + (warp - gx * (gq + 1u)) / gq;
+    const uint32_t gnw = gq + (gi < gx ? 1u : 0u), w0 = gi * gq + min(gi, gx), gw = warp - w0;
+    const WarpGrp grp{tid - 32u * w0, 32u * gnw, 1u + gi};
+    const uint32_t usedG = NG * gWords + 32u * nw;  // all groups' buffers
+    uint32_t* const sD0 = sTile + gi * gWords + 32u * w0;
     uint32_t* const sSpk = sD0 + ncol;
     uint32_t* const sList = sD0 + 2u * ncol;
     uint32_t* const sRed = sD0 + 3u * ncol;  // 192 words and
@@ -575,9 +581,9 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     uint32_t* const sCtl = sHist + 256u;      // 64 words: select control, gated count
     uint32_t* const sH0 = sCtl + 64u;         // the drive histogram
     uint32_t* const sScr = sH0 + kHistWords + 32u * gw;  // this warp's drive recompute sums
-    const bool dbuf = NG == 1u ? gWords + 32u * nw + ncol + kHistWords <= 2u * kItemWords
-                               : NG * (ncol + kHistWords) <= (c.dacc ? 2u : 1u) * accWords;
-    uint32_t* const sD1 = NG == 1u ? sD0 + gWords + 32u * nw : sAcc + gi * (ncol + kHistWords);
+    const bool dbuf = usedG + NG * (ncol + kHistWords) <= avail;
+    const uint32_t usedEnd = usedG + (dbuf ? NG * (ncol + kHistWords) : 0u);
+    uint32_t* const sD1 = sTile + usedG + gi * (ncol + kHistWords);
     uint32_t* const sH1 = sD1 + ncol;
     const uint32_t* hStep = d.thHist + (size_t)(t % 3u) * B * kHistWords;
     auto load_drv = [&](uint32_t b, uint32_t slot) {
@@ -588,23 +594,53 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       uint4* hd = reinterpret_cast<uint4*>(slot ? sH1 : sH0);
       for (uint32_t i = grp.t; i < kHistWords / 4u; i += grp.nt) cp_async16(hd + i, hs + i);
     };
-    // Tasks of worker wid (W = NG per CTA): trajectory wid + k * W for the full rounds k < F.
-    // The R < W trajectories of the last round are split, when each can have at least two
-    // workers, into P = W / R parts, each on a range of whole groups (8 columns): every part
-    // selects the same threshold, then gates, ballots, writes and lists only its own columns,
-    // so the last round costs about one threshold select instead of a whole trajectory.
-    const uint32_t W = gridDim.x * NG, wid = blockIdx.x * NG + gi;
-    const uint32_t F = B / W, R = B - F * W;
-    const uint32_t P = R ? W / R : 0u;
-    const bool split = P >= 2u;
-    const uint32_t ntask = F + (R != 0u && wid < (split ? R * P : R) ? 1u : 0u);
-    auto task_b = [&](uint32_t k) { return k < F ? wid + k * W : F * W + (split ? wid / P : wid); };
+    // Tasks. A worker is one group; workers are numbered group-major (wid = gi * G + CTA), so
+    // whole trajectories spread evenly over the CTAs. A part is a range of whole groups (8
+    // columns) of one trajectory: every part selects the same threshold, then gates, ballots,
+    // writes and lists only its own columns, so a split trajectory costs each of its workers
+    // about one threshold select.
+    // * When the CTAs' groups outnumber B / G whole trajectories each, groups gi < B / G take
+    //   trajectory gi * G + CTA, and the B mod G remaining trajectories are split over the
+    //   other groups (P parts each), which run beside the whole ones.
+    // * Otherwise worker wid takes trajectories wid + k * W for the full rounds k < B / W, and
+    //   the remaining R < W are split into P = W / R parts when P >= 2, else taken whole.
+    const uint32_t G = gridDim.x, W = G * NG, perCta = B / G;
+    const bool spare = perCta < NG && B % G != 0u;
+    uint32_t nfull, fb0, fstep, pb = 0u, ppi = 0u, pnp = 1u;
+    bool hasPart = false;
+    if (spare) {
+      const uint32_t v = (gi - min(gi, perCta)) * G + blockIdx.x, V = (NG - perCta) * G, R = B - perCta * G;
+      const uint32_t P = V / R;
+      fstep = 0u;
+      if (gi < perCta) {
+        nfull = 1u;
+        fb0 = gi * G + blockIdx.x;
+      } else if (P >= 2u) {
+        nfull = 0u;
+        fb0 = 0u;
+        hasPart = v < R * P;
+        pb = perCta * G + v / P; ppi = v % P; pnp = P;
+      } else {
+        nfull = v < R ? 1u : 0u;
+        fb0 = perCta * G + v;
+      }
+    } else {
+      const uint32_t wid = gi * G + blockIdx.x, F = B / W, R = B - F * W;
+      const uint32_t P = R ? W / R : 0u;
+      fb0 = wid;
+      fstep = W;
+      nfull = F + (R != 0u && P < 2u && wid < R ? 1u : 0u);
+      hasPart = P >= 2u && wid < R * P;
+      pb = F * W + (P ? wid / P : 0u); ppi = P ? wid % P : 0u; pnp = P ? P : 1u;
+    }
+    const uint32_t ntask = nfull + (hasPart ? 1u : 0u);
+    auto task_b = [&](uint32_t k) { return k < nfull ? fb0 + k * fstep : pb; };
     if (ntask) load_drv(task_b(0), 0);
     cp_async_commit();
     for (uint32_t k = 0; k < ntask; ++k) {
       const uint32_t b = task_b(k);
-      const bool part = split && k == F;
-      const uint32_t pi = part ? wid % P : 0u, np = part ? P : 1u;
+      const bool part = k >= nfull;
+      const uint32_t pi = part ? ppi : 0u, np = part ? pnp : 1u;
       const uint32_t gLo = pi * ngrp / np, gHi = (pi + 1u) * ngrp / np, cLo = 8u * gLo, cHi = 8u * gHi;
       const uint32_t slot = dbuf ? (k & 1u) : 0u;
       uint32_t* sD = slot ? sD1 : sD0;
@@ -736,10 +772,10 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       if (!dbuf && hasNext) load_drv(task_b(k + 1u), 0);  // committed at the next task's start
     }
     cp_async_wait<0>();
-    // second drive buffers in the counter region: zero again before the next phase 1
-    if (NG == 2u && dbuf) {
+    // the part of the counter region that phase 2 used: zero again before the next phase 1
+    if (usedEnd > 2u * kItemWords) {
       __syncthreads();
-      for (uint32_t i = tid; i < NG * (ncol + kHistWords); i += blockDim.x) sAcc[i] = 0u;
+      for (uint32_t i = tid; i < usedEnd - 2u * kItemWords; i += blockDim.x) sAcc[i] = 0u;
     }
     if (t + 1u < c.T && !grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;
   }
