@@ -85,45 +85,30 @@ __device__ __forceinline__ void bs_clip(uint32_t& a0, uint32_t& a1, uint32_t& a2
 // ---------------------------------------------------------------- exact k-of-32
 // rank = #{j : v_j > v_i or (v_j == v_i and j < i)}; winners rank < k; vk / vk1 are the
 // values ranked k-1 and k (0 if no lane has that rank). src/axon.mm:134-144.
-// Method, for values below 2^27: the key (v << 5) | (31 - lane) is unique per lane and orders
-// the lanes exactly as the rank does, so a lane's rank is the number of larger keys among
-// the 32 (independent shuffle-compares, no dependent chain), and vk, vk1 are the values of
-// the lanes ranked k-1 and k. Larger values: the value ranked k-1 by a most-significant-bit-
-// first radix select over the bits of the largest value, with the lanes that still match the
-// selected prefix kept as a ballot mask; then every lane above it wins, and of the lanes
-// equal to it the lowest ones fill the remaining places.
+// Method: a bit-sliced comparison. Over the significant bits of the largest value, most
+// significant first, one ballot per bit; each lane keeps the lanes whose values are larger
+// than its own (gt) and those equal so far (eq): a lane holding 0 at a bit moves the equal
+// lanes holding 1 there into gt and drops them from eq, a lane holding 1 drops the equal
+// lanes holding 0. Then rank = popc(gt) + the equal lanes below it. The ballots do not
+// depend on one another; each lane's update chain is a few integer operations per bit.
 __device__ __forceinline__ uint32_t warp_kwta(uint32_t v, uint32_t lane, uint32_t k, uint32_t& vk, uint32_t& vk1) {
   if (k == 0u) { vk = 0u; vk1 = __reduce_max_sync(kFull, v); return 0u; }
   if (k > 32u) { vk = 0u; vk1 = 0u; return kFull; }
-  if (__all_sync(kFull, v < (1u << 27))) {
-    const uint32_t key = (v << 5) | (31u - lane);
-    uint32_t r0 = 0u, r1 = 0u;
-#pragma unroll
-    for (int j = 0; j < 32; j += 2) {
-      r0 += __shfl_sync(kFull, key, j) > key ? 1u : 0u;
-      r1 += __shfl_sync(kFull, key, j + 1) > key ? 1u : 0u;
-    }
-    const uint32_t rank = r0 + r1;
-    vk = __shfl_sync(kFull, v, __ffs(__ballot_sync(kFull, rank == k - 1u)) - 1);
-    vk1 = k == 32u ? 0u : __shfl_sync(kFull, v, __ffs(__ballot_sync(kFull, rank == k)) - 1);
-    return __ballot_sync(kFull, rank < k);
-  }
   const uint32_t M = __reduce_max_sync(kFull, v);
-  uint32_t m = kFull, prefix = 0u, rem = k;
+  uint32_t gt = 0u, eq = kFull;
   for (int bit = (int)(32u - __clz(M)) - 1; bit >= 0; --bit) {
-    const uint32_t ones = m & __ballot_sync(kFull, (v >> bit) & 1u);
-    const uint32_t c1 = (uint32_t)__popc(ones);
-    if (c1 >= rem) { m = ones; prefix |= 1u << bit; } else { rem -= c1; m &= ~ones; }
+    const uint32_t ones = __ballot_sync(kFull, (v >> bit) & 1u);
+    if ((v >> bit) & 1u) {
+      eq &= ones;
+    } else {
+      gt |= eq & ones;
+      eq &= ~ones;
+    }
   }
-  vk = prefix;
-  const uint32_t gt = __ballot_sync(kFull, v > prefix), eq = __ballot_sync(kFull, v == prefix);
-  const uint32_t ngt = (uint32_t)__popc(gt), need = k - ngt;  // 1 <= need <= popc(eq)
-  const uint32_t pos = __fns(eq, 0u, (int)need);               // the need-th lowest lane equal to vk
-  const uint32_t low = eq & ((2u << pos) - 1u);
-  if (k == 32u) vk1 = 0u;
-  else if (ngt + (uint32_t)__popc(eq) > k) vk1 = prefix;
-  else vk1 = __reduce_max_sync(kFull, v < prefix ? v : 0u);
-  return gt | low;
+  const uint32_t rank = (uint32_t)__popc(gt) + (uint32_t)__popc(eq & ((1u << lane) - 1u));
+  vk = __shfl_sync(kFull, v, __ffs(__ballot_sync(kFull, rank == k - 1u)) - 1);
+  vk1 = k == 32u ? 0u : __shfl_sync(kFull, v, __ffs(__ballot_sync(kFull, rank == k)) - 1);
+  return __ballot_sync(kFull, rank < k);
 }
 
 // ---------------------------------------------------------------- asynchronous copies

@@ -235,8 +235,8 @@ def test_dense_activity_overflows_tile_pool(target, inbr):
 
 
 def test_kwta_kat_gpu():
-    """The kernels' k-of-32 equals the oracle's on ties, spread and large values (the rank-
-    count form below 2^27, the radix select above) for every k from 0 to 33."""
+    """The kernels' k-of-32 (bit-sliced rank) equals the oracle's on ties, spread values and
+    values up to 2^32 - 1, for every k from 0 to 33."""
     import axon_b200 as ax
     from test_oracle_pins import kwta_cases
 
