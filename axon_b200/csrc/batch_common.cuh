@@ -10,9 +10,10 @@
 namespace axon {
 
 // Tile layout for the batched kernel: word w of row r of a (column, branch) tile is stored
-// at w*32 + ((r + 4w) mod 32). Rows r..r+3 (r a multiple of 4) of one word are then 16
-// contiguous bytes, and lanes reading different words hit different groups of 4 banks.
-__host__ __device__ __forceinline__ uint32_t w3r_pos(uint32_t r, uint32_t w) { return w * 32u + ((r + 4u * w) & 31u); }
+// at w*32 + (r XOR 4w). Rows r..r+3 (r a multiple of 4) of one word are then 16 contiguous
+// bytes, lanes reading different words hit different groups of 4 banks, and the offset
+// never wraps, so each read's address is one XOR and one add from the word's base.
+__host__ __device__ __forceinline__ uint32_t w3r_pos(uint32_t r, uint32_t w) { return w * 32u + (r ^ (4u * w)); }
 
 // ---------------------------------------------------------------- TMA bulk copy + mbarrier
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -71,7 +72,7 @@ __device__ __forceinline__ void acc_add4c(uint32_t* accb, uint32_t r, uint32_t c
                                           uint32_t dthr, uint32_t bst) {
   if (PACK) {
     const uint32_t k = (0x8000u - min(dthr, 0x8000u)) * 0x00010001u;
-    const uint32_t p0 = c0 | (c1 << 16), p1 = c2 | (c3 << 16);
+    const uint32_t p0 = c0 + (c1 << 16), p1 = c2 + (c3 << 16);
     const uint32_t n0 = ((p0 + k) >> 15) & 0x00010001u, n1 = ((p1 + k) >> 15) & 0x00010001u;
     atomicAdd(accb + (r >> 1), LIN ? p0 + bst * n0 : n0);
     atomicAdd(accb + (r >> 1) + 1, LIN ? p1 + bst * n1 : n1);
