@@ -100,12 +100,12 @@ def test_recall_batched_equals_plain_full_geometry():
 
 @pytest.mark.parametrize("B", [149, 320, 400])
 def test_recall_several_trajectories_per_cta(B):
-    """More trajectories than CTAs (one per SM, 148 on a B200): a CTA selects the
-    thresholds of two or three trajectories in turn, the next one's drives loading while
-    the current one is processed. At 400 trajectories two counter buffers no longer fit in
-    shared memory, and phase 1 keeps one with a second barrier per item. Every trajectory
-    equals the plain method; a sample, including trajectories of a CTA's second and third
-    turn, equals the oracle."""
+    """More trajectories than CTAs (one per SM, 148 on a B200): a CTA's warp groups each
+    select the threshold of a trajectory of their own, some groups taking a second whole
+    trajectory or a part of one, the next one's drives loading while the current one is
+    processed. At 400 trajectories two counter buffers no longer fit in shared memory, and
+    phase 1 keeps one with a second barrier per item. Every trajectory equals the plain
+    method; a sample, including later trajectories, equals the oracle."""
     cfg, gpu, cpu, pats = trained_pair({}, 6, 3, 16)
     cues = make_cues(pats, cfg.ncol, B, np.random.default_rng(B))
     rb = gpu.recall(cues, 20, 5, hist=True, stats=True)
@@ -232,3 +232,19 @@ def test_slab_policies_full_geometry(contraction):
     for s in ("floor", "floor_always"):
         assert np.array_equal(runs[s]["hist"], runs["full"]["hist"]), s
         assert np.array_equal(runs[s]["stats"], runs["full"]["stats"]), s
+
+
+@pytest.mark.parametrize("B,T,clamp", [(1, 1, 1), (5, 1, 0), (9, 7, 0), (9, 6, 6), (37, 12, 2), (530, 6, 3)])
+def test_recall_edge_shapes(B, T, clamp):
+    """One-step readouts, no clamped step, every step clamped, the afferent cache's shortest
+    clamp (2 steps), and more trajectories than one launch holds (512: the host splits the
+    batch): the batched method equals the plain one on every trajectory and step, and a
+    sample equals the oracle."""
+    cfg, gpu, cpu, pats = trained_pair({}, 6, 3, 16)
+    cues = make_cues(pats, cfg.ncol, B, np.random.default_rng(B + T))
+    rb = gpu.recall(cues, T, clamp, hist=True, stats=True)
+    rp = gpu.recall(cues, T, clamp, hist=True, stats=True, method="plain")
+    assert np.array_equal(rb["hist"], rp["hist"]) and np.array_equal(rb["final"], rp["final"])
+    idx = sorted({0, B // 2, B - 1})
+    f, h, _, _ = oracle_runs(cpu, cues[idx], T, clamp, 0)
+    assert np.array_equal(rb["hist"][idx], h) and np.array_equal(rb["final"][idx], f)
