@@ -257,6 +257,8 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   uint32_t uses0 = 0, uses1 = 0;  // completed phases per buffer
   uint32_t kbuf = 0;              // buffer of the next item
   uint32_t epoch = 0;
+  uint32_t claim = 0;             // thread 0: the item claimed one ahead
+  bool pre = false;               // the step's first item was claimed and its tiles issued already
 
   auto issue = [&](uint32_t item, uint32_t buf) {  // thread 0 only
     const uint32_t c0 = item * kRecallCpi;
@@ -345,17 +347,22 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     for (uint32_t b = tid; b < B; b += blockDim.x) sFloor[b] = hist_floor(d.thPrev + b);  // read after the sync below
 
     // ---------------- phase 1
-    // thread 0 claims one item ahead: the claim's round trip overlaps the current item
-    uint32_t claim = nitems;
+    // thread 0 claims one item ahead: the claim's round trip overlaps the current item. After
+    // the first step the first item was claimed, and its tiles requested, before the grid
+    // barrier that ended the previous step.
     if (tid == 0) {
-      const uint32_t it0 = atomicAdd(d.work + t, 1u);
-      sMisc[1] = it0;
-      sMisc[6] = sMisc[7] = 0u;
-      if (it0 < nitems) {
-        issue(it0, kbuf);
-        claim = atomicAdd(d.work + t, 1u);
+      if (!pre) {
+        const uint32_t it0 = atomicAdd(d.work + t, 1u);
+        sMisc[1] = it0;
+        claim = nitems;
+        if (it0 < nitems) {
+          issue(it0, kbuf);
+          claim = atomicAdd(d.work + t, 1u);
+        }
       }
+      sMisc[6] = sMisc[7] = 0u;
     }
+    pre = false;
     __syncthreads();
     uint32_t item = sMisc[1];
     if (warp == 0 && item < nitems) prep(item, kbuf, c1In, cMIn);
@@ -772,12 +779,30 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       if (!dbuf && hasNext) load_drv(task_b(k + 1u), 0);  // committed at the next task's start
     }
     cp_async_wait<0>();
+    if (t + 1u == c.T) break;
     // the part of the counter region that phase 2 used: zero again before the next phase 1
-    if (usedEnd > 2u * kItemWords) {
-      __syncthreads();
-      for (uint32_t i = tid; i < usedEnd - 2u * kItemWords; i += blockDim.x) sAcc[i] = 0u;
+    __syncthreads();
+    for (uint32_t i = tid; i + 2u * kItemWords < usedEnd; i += blockDim.x) sAcc[i] = 0u;
+    // The tiles of the next step's first item do not depend on this step's spikes: claim it
+    // and request them now (the phase-2 buffers over the tile region are free after the
+    // barrier above), so that the copy runs while the grid barrier waits.
+    if (tid == 0) {
+      const uint32_t it0 = atomicAdd(d.work + t + 1u, 1u);
+      sMisc[1] = it0;
+      claim = nitems;
+      if (it0 < nitems) {
+        issue(it0, kbuf);
+        claim = atomicAdd(d.work + t + 1u, 1u);
+      }
     }
-    if (t + 1u < c.T && !grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) return;
+    pre = true;
+    if (!grid_barrier(d.bar, d.err, gridDim.x, epoch++, c.waitNs, sMisc)) {
+      // the copy requested above must land before the CTA's shared memory is released
+      if (tid == 0 && sMisc[1] < nitems)
+        mbar_wait(&sBar[kbuf], (kbuf ? uses1 : uses0) & 1u, c.waitNs > kDrainNs ? c.waitNs : kDrainNs);
+      __syncthreads();
+      return;
+    }
   }
 }
 
