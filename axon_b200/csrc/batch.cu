@@ -17,11 +17,14 @@
 //            cost nothing. The counters then become the per-neuron and column drives, and
 //            the write-back that reads them clears them. One CTA barrier per item separates
 //            its units from its write-back; with two counter buffers nothing else does.
-//            The write-back also counts every recurrent column drive into the trajectory's
-//            drive histogram for the step (count, largest and smallest drive per bin).
-//   phase 2  per trajectory: the column threshold from that histogram (hist_theta), the
-//            exact k-of-32 ballot only for columns that pass the gate, the new spike
-//            vector, and its group lists.
+//            The write-back also counts every recurrent column drive at or above the
+//            trajectory's floor into its drive histogram for the step (count, largest and
+//            smallest drive per bin), and stores the per-neuron drives of those columns.
+//   phase 2  per trajectory, by groups of warps that each take trajectories of their own:
+//            the column threshold from that histogram (hist_theta, or a sorting select when
+//            too few drives reached the floor), the exact k-of-32 ballot only for columns
+//            that pass the gate, the new spike vector, and its group lists. The tiles of
+//            the next step's first item are requested before the grid barrier.
 #include <cstdint>
 
 #include "axon_device.cuh"
