@@ -79,7 +79,9 @@ axon_status axon_net::recall(const uint32_t* cues, uint32_t B, const axon_recall
     char* p = (char*)io.p;
     auto take = [&](size_t bytes) { uint32_t* r = (uint32_t*)p; p += al(bytes); return r; };
     uint32_t* c = take(bn * 4);
-    CK(cudaMemcpyAsync(c, cues, bn * 4, cudaMemcpyHostToDevice, stream));
+    // the clamp reads a cue's input columns only (the first incols words of each row)
+    if (cfg.incols > 0)
+      CK(cudaMemcpy2DAsync(c, ncol * 4, cues, ncol * 4, cfg.incols * 4, B, cudaMemcpyHostToDevice, stream));
     dCues = c;
     if (refBall) {
       uint32_t* r = take(bn * 4);

@@ -707,7 +707,8 @@ def main() -> None:
                                  "of every active (column, branch, trajectory)) per second, against 16 popcounts per SM "
                                  "per clock at the sampled SM clock; ncu's XU-pipe utilisation is the same measure"},
         "cpu_baseline": cpu,
-        "e2e": {"value": world * events / e2e_s, "unit": "synaptic events/s", "h2d_bytes_per_step": int(cues.nbytes),
+        "e2e": {"value": world * events / e2e_s, "unit": "synaptic events/s",
+                "h2d_bytes_per_step": int(B * INCOLS * 4),  # the cues' input columns: all the clamp reads
                 "d2h_bytes_per_step": int(B * NCOL * 4)},
         "wave_variant": wave,
         "contraction_ab": contraction,

@@ -158,7 +158,9 @@ uint32_t axon_noisy_cue_seed(uint32_t q, uint32_t pct, uint32_t draw);
 
 /* ---------------------------------------------------------------- batched readout
  * B readout trajectories of one network, each exactly what present() with learn = 0 does
- * (src/axon.mm:815-888): `cues` holds B clamp patterns of ncol words. The batched method
+ * (src/axon.mm:815-888): `cues` holds B clamp patterns of ncol words, of which only the
+ * first incols (the input columns the clamp sets) are read, and axon_recall copies only
+ * those to the device. The batched method
  * runs all B in one launch that reads each W3 tile once for every trajectory; the plain
  * method runs them one presentation at a time (same results, for comparison). Outputs
  * are optional (NULL to skip): final_spk B*ncol spikes of the last step, hist B*T*ncol
