@@ -516,10 +516,10 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
 #pragma unroll
           for (int i = 0; i < 16; ++i) s += w[i] - 65535u * (w[i] >> 16);
           const uint32_t fl = sFloor[b];
-          if (storeAll || s >= fl) {
-            uint4* dst = reinterpret_cast<uint4*>(d.acc) + ((size_t)b * ncol + col) * 4u;
+          if (storeAll || s >= fl) {  // laid out [column][quad][trajectory], like the afferent cache
+            uint4* dst = reinterpret_cast<uint4*>(d.acc) + (size_t)col * 4u * B + b;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) dst[j] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
+            for (int j = 0; j < 4; ++j) dst[(size_t)j * B] = make_uint4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
           }
           __stcg(d.drv + (size_t)b * ncol + col, s);
           if (col >= incols && s >= fl) count_drive(d.thHist + ((size_t)(t % 3u) * B + b) * kHistWords, s);
@@ -730,7 +730,10 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
           const uint32_t e = e0 + u * gnw;
           av[u] = 0u;
           if (e < npend && sD[sList[e]] >= reFloor) {
-            const size_t o = ((size_t)b * ncol + sList[e]) * 32u + lane;
+            // the fast write-back's layout: neuron n of (column cc, trajectory b) is 16-bit
+            // element n % 8 of quad ((cc * 4 + n / 8) * B + b); the others [b][cc][neuron]
+            const size_t o = fast ? (((size_t)sList[e] * 4u + (lane >> 3)) * B + b) * 8u + (lane & 7u)
+                                  : ((size_t)b * ncol + sList[e]) * 32u + lane;
             av[u] = c.acc32 ? __ldcg(reinterpret_cast<const uint32_t*>(d.acc) + o)
                             : (uint32_t)__ldcg(reinterpret_cast<const uint16_t*>(d.acc) + o);
           }

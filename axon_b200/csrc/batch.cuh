@@ -23,9 +23,10 @@ struct RecallDev {
   uint4* entM;              // [2][ngrp][B] per-group lists of trajectories with several nonzero words
   uint32_t* ecnt;           // [2 parity][2 lists][ngrp] list lengths (parity 0 zeroed before launch)
   uint32_t* drv;            // [B][ncol] column drives of the current step
-  void* acc;                // [B][ncol][32] per-neuron drive (u16 or u32) of the current step; on the packed
-                            // path without bias, facilitation or drive log only the entries whose column
-                            // drive reaches the trajectory's histogram floor are written
+  void* acc;                // per-neuron drives (u16 or u32) of the current step, [B][ncol][32]; on the packed
+                            // path without bias, facilitation or drive log laid out [ncol][4][B] x 8 u16, and
+                            // only the entries whose column drive reaches the trajectory's histogram floor
+                            // are written
   uint32_t* finalOut;       // [B][ncol] spikes of the last step, or null
   uint32_t* hist;           // [B][T][ncol] spikes of every step, or null
   uint32_t* stats;          // [B][1024] counters (zeroed before launch), or null
