@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   uint32_t* sP1 = sConn + 2 * 64;                        // [2][68] single-word entries: prefix over 64 branches
   uint32_t* sPM = sP1 + 2 * 68;                          // [2][68] multi-word entries
   uint32_t* sPC = sPM + 2 * 68;                          // [2][68] MMA: chunks of 8 entries, prefix over branches
-  uint32_t* sMisc = sPC + 2 * 68;  // [16]: grid barrier flag, first item, -, -, gated count, -, unit counters [2], next items [2]
+  uint32_t* sMisc = sPC + 2 * 68;  // [16]: grid barrier flag, first item, -, -, -, -, unit counters [2], next items [2]
   uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
   uint32_t* sFloor = sMisc + 20;  // [B] each trajectory's histogram floor for this step
 
