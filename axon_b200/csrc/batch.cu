@@ -722,7 +722,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
       }
       // the others from the slab, a warp's gated columns kPend at a time: their per-neuron
       // drives load together
-      constexpr uint32_t kPend = 8;
+      constexpr uint32_t kPend = 4;
       for (uint32_t e0 = gw; e0 < npend; e0 += kPend * gnw) {
         uint32_t av[kPend];
 #pragma unroll
