@@ -246,6 +246,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
   uint32_t* sMisc = sPC + 2 * 68;  // [16]: grid barrier flag, first item, -, -, -, -, unit counters [2], next items [2]
   uint64_t* sBar = reinterpret_cast<uint64_t*>(sMisc + 16);  // [2]
   uint32_t* sFloor = sMisc + 20;  // [B] each trajectory's histogram floor for this step
+  uint32_t* sUT = sFloor + B;     // [2][kUnitTab] first branch of each list per unit (prep)
 
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nw = blockDim.x >> 5;
   const uint32_t nitems = (ncol + kRecallCpi - 1) / kRecallCpi;
@@ -311,6 +312,39 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
     PM[1 + lane] = m0;
     PM[33 + lane] = totM + m1;
     if (lane == 0) P1[0] = PM[0] = 0u;
+    // Unit table: for unit u < kUnitTab, the number of branches of each list that end at or
+    // before the unit's first entry of that list (multi-word in the low half, single-word in
+    // the high half), which the units would otherwise count with four ballots each. A branch
+    // ending at prefix e is counted from unit ceil(e / 32) on (single-word entries follow
+    // all EM multi-word ones): a histogram over units, then a prefix sum. Where a unit
+    // straddles the two lists the single-word count is a lower bound, which the units' step
+    // over branch boundaries completes.
+    uint32_t* UT = sUT + buf * kUnitTab;
+    for (uint32_t u = lane; u < kUnitTab; u += 32u) UT[u] = 0u;
+    __syncwarp();
+    const uint32_t EMt = __shfl_sync(kFull, totM + m1, 31);
+    const uint32_t uM0 = (m0 + 31u) >> 5, uM1 = (totM + m1 + 31u) >> 5;
+    const uint32_t uS0 = (a0 + EMt + 31u) >> 5, uS1 = (totA + a1 + EMt + 31u) >> 5;
+    if (uM0 < kUnitTab) atomicAdd(UT + uM0, 1u);
+    if (uM1 < kUnitTab) atomicAdd(UT + uM1, 1u);
+    if (uS0 < kUnitTab) atomicAdd(UT + uS0, 1u << 16);
+    if (uS1 < kUnitTab) atomicAdd(UT + uS1, 1u << 16);
+    __syncwarp();
+    {  // inclusive prefix over the kUnitTab units, kUnitTab / 32 per lane (counts <= 64 per half)
+      constexpr uint32_t kPerLane = kUnitTab / 32u;
+      uint32_t v[kPerLane], sum = 0u;
+#pragma unroll
+      for (uint32_t j = 0; j < kPerLane; ++j) { sum += UT[lane * kPerLane + j]; v[j] = sum; }
+      uint32_t before = sum;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t x = __shfl_up_sync(kFull, before, off);
+        if (lane >= (uint32_t)off) before += x;
+      }
+      before -= sum;
+#pragma unroll
+      for (uint32_t j = 0; j < kPerLane; ++j) UT[lane * kPerLane + j] = v[j] + before;
+    }
   };
 
   for (uint32_t t = 0; t < c.T; ++t) {
@@ -420,10 +454,17 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         // of that list: the number of branches ending at or before it; a lane then steps over
         // the few branch boundaries between that entry and its own
         const uint32_t f0 = u * 32u, fM = min(f0, EM), f1 = f0 > EM ? f0 - EM : 0u;
-        const uint32_t spM = (uint32_t)__popc(__ballot_sync(kFull, cPM[lane + 1] <= fM)) +
-                             (uint32_t)__popc(__ballot_sync(kFull, cPM[lane + 33] <= fM));
-        const uint32_t sp1 = (uint32_t)__popc(__ballot_sync(kFull, cP1[lane + 1] <= f1)) +
-                             (uint32_t)__popc(__ballot_sync(kFull, cP1[lane + 33] <= f1));
+        uint32_t spM, sp1;
+        if (u < kUnitTab) {  // from the item's unit table
+          const uint32_t ut = sUT[bcur * kUnitTab + u];
+          spM = ut & 0xFFFFu;
+          sp1 = ut >> 16;
+        } else {
+          spM = (uint32_t)__popc(__ballot_sync(kFull, cPM[lane + 1] <= fM)) +
+                (uint32_t)__popc(__ballot_sync(kFull, cPM[lane + 33] <= fM));
+          sp1 = (uint32_t)__popc(__ballot_sync(kFull, cP1[lane + 1] <= f1)) +
+                (uint32_t)__popc(__ballot_sync(kFull, cP1[lane + 33] <= f1));
+        }
         uint32_t flat = f0 + lane;
         if (flat >= E) continue;
         const bool single = flat >= EM;
@@ -815,7 +856,8 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
 size_t recall_smem_bytes(uint32_t ncol, uint32_t B, uint32_t acc32, uint32_t dacc) {
   (void)ncol;
   const size_t stride = acc32 ? 33 : 17;
-  return (2ull * kItemWords + (dacc ? 2 : 1) * kRecallCpi * (size_t)B * stride + 2 * (64 + 68 + 68 + 68) + 16 + 4 + B) *
+  return (2ull * kItemWords + (dacc ? 2 : 1) * kRecallCpi * (size_t)B * stride + 2 * (64 + 68 + 68 + 68) + 16 + 4 + B +
+          2 * kUnitTab) *
          4;
 }
 

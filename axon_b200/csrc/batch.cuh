@@ -9,6 +9,7 @@ namespace axon {
 constexpr uint32_t kRecallMaxB = 512;   // trajectories per launch (the host splits larger batches)
 constexpr uint32_t kRecallCpi = 2;      // columns per phase-1 work item
 constexpr uint32_t kRecallMaxT = 1024;  // steps of a batched readout without per-step records
+constexpr uint32_t kUnitTab = 128;      // phase-1 units per work item with a precomputed start branch
 
 // Device buffers of one batched recall launch over B trajectories of one network.
 struct RecallDev {
