@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
           claim = atomicAdd(d.work + t, 1u);
         }
       }
-      sMisc[6] = sMisc[7] = 0u;
+      sMisc[6] = sMisc[7] = MMA ? 0u : nw - 1u;  // unit counters (see the unit loop)
     }
     pre = false;
     __syncthreads();
@@ -445,10 +445,16 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         mma_units<PACK, LIN>(sPC + bcur * 68u, cP1, cPM, cConn, tileBase, accB, accStride, sMisc + 6 + bcur, e1In,
                              eMIn, spkIn, B, ncol, dthr, bst, lane);
       } else
-      for (;;) {
-        uint32_t u = 0;
-        if (lane == 0) u = atomicAdd(sMisc + 6 + bcur, 1u);
-        u = __shfl_sync(kFull, u, 0);
+      // the first unit of warps 1.. is fixed (unit warp - 1, no claim round trip); later units,
+      // and all of warp 0's (it joins after its look-ahead), are claimed from the counter,
+      // which starts at nw - 1
+      for (bool first = warp != 0u;; first = false) {
+        uint32_t u = warp - 1u;
+        if (!first) {
+          u = 0;
+          if (lane == 0) u = atomicAdd(sMisc + 6 + bcur, 1u);
+          u = __shfl_sync(kFull, u, 0);
+        }
         if (u >= units) break;
         // the branch of each list (multi-word, single-word) that holds the unit's first entry
         // of that list: the number of branches ending at or before it; a lane then steps over
@@ -522,7 +528,7 @@ __global__ void __launch_bounds__(896, 1) k_recall(RecallDev d, RecallCfg c) {
         __syncthreads();
         return;
       }
-      if (tid == 0) sMisc[6 + bcur] = 0u;  // every warp has claimed its units of this item
+      if (tid == 0) sMisc[6 + bcur] = MMA ? 0u : nw - 1u;  // every warp has claimed its units of this item
       // per-neuron and column drives of the item's columns for every trajectory
       if (fast) {
         // the packed counters already are the u16 drive slab. One (column, trajectory) pair
