@@ -248,3 +248,31 @@ def test_recall_edge_shapes(B, T, clamp):
     idx = sorted({0, B // 2, B - 1})
     f, h, _, _ = oracle_runs(cpu, cues[idx], T, clamp, 0)
     assert np.array_equal(rb["hist"][idx], h) and np.array_equal(rb["final"][idx], f)
+
+
+def test_recall_refuses_bad_arguments():
+    """The recall refuses, with AXON_EINVAL and before any copy or launch, an unknown slab
+    policy or contraction unit, T = 0, T above 64 with per-step records or above 1024
+    without, and B = 0; the network stays usable."""
+    import ctypes as C
+
+    import axon_b200._capi as A
+
+    cfg, gpu, cpu, pats = trained_pair({}, 2, 1, 16)
+    cues = make_cues(pats, cfg.ncol, 3, np.random.default_rng(9))
+    final = np.zeros_like(cues)
+    for fields in (dict(slab=3), dict(contraction=2), dict(T=0)):
+        a = A.RecallArgs(T=fields.get("T", 10), clamp_steps=5, slab=fields.get("slab", 0),
+                         contraction=fields.get("contraction", 0))
+        st = A.lib().axon_recall(gpu._h, cues.ctypes.data_as(C.c_void_p), 3, C.byref(a), None,
+                                 final.ctypes.data_as(C.c_void_p), None, None, None, None)
+        assert st == A.AXON_EINVAL, fields
+    for T, hist in ((65, True), (1025, False)):
+        with pytest.raises(A.AxonError) as e:
+            gpu.recall(cues, T, 5, hist=hist)
+        assert e.value.status == A.AXON_EINVAL
+    with pytest.raises(A.AxonError) as e:
+        gpu.recall(cues[:0], 10, 5)
+    assert e.value.status == A.AXON_EINVAL
+    f, _, _, _ = oracle_runs(cpu, cues[:1], 10, 5, 0)
+    assert np.array_equal(gpu.recall(cues, 10, 5)["final"][:1], f)
